@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Throughput of the CUDA Kirchhoff PSTM backend, in migrated sample-trace pairs/s.
+
+Workload (default ``c2tile``): the production-tile case -- 1,048,576 traces of
+1500 samples at 2 ms with random source/receiver positions in a 3.2 x 3.2 km
+patch, output bins of 12.5 m with 1500 samples at 2 ms, laterally varying
+v_rms(t,x,y), triangle AA on, reference default 5 km aperture (every trace is
+inside it).  One step is one ``migrate_tile`` call: a 64 x 64-pillar tile of the
+256 x 256 output grid against the whole trace panel (6.44e12 sample-trace
+pairs), the unit of work the reference executor hands a backend.  Successive
+steps walk the 16 tiles of the grid; with N GPUs rank r takes tiles r, r+N, ...
+(disjoint outputs, no collective on the data path: weak scaling).
+
+``value``      device-resident inputs, timed with CUDA events on the launch stream.
+``e2e``        through the public backend (``CudaKernel.migrate_tile``) with
+               pinned host arrays: every step copies the panel, geometry,
+               velocity and image/fold in and the image/fold out.
+``cpu_baseline`` the FP64 CPU oracle (a port of the reference algorithm) on a
+               bounded sample of the same workload, on this host's cores.
+``--impl reference`` times that CPU port alone, as the reference arm.
+
+Inputs are larger than L2 (the FP32 panel is 6.3 GB), so no L2 flush is needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "migrated sample-trace pairs/s"
+UNIT = "pairs/s"
+
+# algorithmic work per sample-trace pair of the straight-ray kernel with AA on
+# (16 FP32 FLOP + 3 MUFU for DSR, interpolation and weights; AA adds 4 + 1)
+FLOP_PER_PAIR = 20
+MUFU_PER_PAIR = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dtype", choices=["f32", "bf16", "f16"], default="f32")
+    ap.add_argument("--traces", type=int, default=1 << 20)
+    ap.add_argument("--tile", type=int, default=64)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ workload
+GRID, NT, NS, DT_MS, DX = 256, 1500, 1500, 2.0, 12.5
+
+
+def tiles_of(tile):
+    n = GRID // tile
+    return [(i * tile, (i + 1) * tile, j * tile, (j + 1) * tile) for i in range(n) for j in range(n)]
+
+
+def config():
+    from pstm_b200 import workloads
+    return workloads.survey_config(kernel_type="straight_ray", aa=True, dx=DX)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample(sv, cfg, tile, n_traces, pillars_x, pillars_y, amps_host):
+    """Time the FP64 oracle on pillars [0:px, 0:py] of the first tile x n_traces."""
+    from oracle import oracle
+    from pstm_b200.base import create_trace_block
+    ix0, _, iy0, _ = tile
+    out, vel = sv.tile(ix0, ix0 + pillars_x, iy0, iy0 + pillars_y)
+    tb = create_trace_block(amps_host[:n_traces], sv.s[:n_traces, 0], sv.s[:n_traces, 1],
+                            sv.r[:n_traces, 0], sv.r[:n_traces, 1], sample_rate_ms=DT_MS)
+    t0 = time.perf_counter()
+    oracle.migrate(tb, out, vel, cfg)
+    dt = time.perf_counter() - t0
+    pairs = pillars_x * pillars_y * NT * n_traces
+    return pairs / dt, pairs, dt
+
+
+def reference_arm(args):
+    """The reference algorithm on the host cores (the CPU port), rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    from pstm_b200 import workloads
+    oracle.build()
+    n_tr = 1 << 18
+    sv = workloads.survey(n_tr, GRID, GRID, NT, DT_MS, NS, dx=DX, seed=7)
+    cfg = config()
+    tile = tiles_of(args.tile)[0]
+    cores = os.cpu_count()
+    px, py = 4, 4
+    for _ in range(args.warmup):
+        cpu_sample(sv, cfg, tile, n_tr, px, py, sv.amps)
+    rates, secs = [], 0.0
+    for _ in range(args.steps):
+        r, pairs, dt = cpu_sample(sv, cfg, tile, n_tr, px, py, sv.amps)
+        rates.append(r)
+        secs += dt
+    value = args.steps * pairs / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "case-2 production tile (256x256x1500 @12.5 m/2 ms, 1,048,576 traces x 1500, "
+                               "3-D v_rms, AA on), CPU sample per step", "parallelism": "openmp"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{px}x{py} pillars x {NT} samples x {n_tr} traces per step (FP64 C port "
+                                   "of the reference Numba/Metal semantics, OpenMP, all host threads)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def main_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from pstm_b200 import build, workloads
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    build.build()
+
+    tdtype = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[args.dtype]
+    N = args.traces
+    sv, amps = workloads.survey_device(N, GRID, GRID, NT, DT_MS, NS, dx=DX, seed=7, dtype=tdtype)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    geo = {k: dev(v) for k, v in (("source_x", sv.s[:, 0]), ("source_y", sv.s[:, 1]),
+                                  ("receiver_x", sv.r[:, 0]), ("receiver_y", sv.r[:, 1]),
+                                  ("midpoint_x", (sv.s[:, 0] + sv.r[:, 0]) / 2.0),
+                                  ("midpoint_y", (sv.s[:, 1] + sv.r[:, 1]) / 2.0))}
+    offset = dev(np.hypot(sv.r[:, 0] - sv.s[:, 0], sv.r[:, 1] - sv.s[:, 1]))
+    tb = TraceBlock(amplitudes=amps, offset=offset, sample_rate_ms=DT_MS, start_time_ms=0.0, **geo)
+    cfg = config()
+    tiles = tiles_of(args.tile)
+    my_tiles = [tiles[(rank + j * world) % len(tiles)] for j in range(args.warmup + args.steps)]
+    T = args.tile
+    img = torch.zeros((T, T, NT), dtype=torch.float64, device="cuda")
+    fold = torch.zeros((T, T, NT), dtype=torch.int32, device="cuda")
+    t_axis = dev(sv.t_axis_ms)
+    tile_args = {}
+    for tl in set(my_tiles):
+        ix0, ix1, iy0, iy1 = tl
+        tile_args[tl] = (OutputTile(image=img, fold=fold, x_axis=dev(sv.x_axis[ix0:ix1]),
+                                    y_axis=dev(sv.y_axis[iy0:iy1]), t_axis_ms=t_axis),
+                         VelocitySlice(vrms=dev(sv.velocity(ix0, ix1, iy0, iy1)), is_1d=False))
+    k = CudaKernel()
+    k.initialize(cfg)
+    pairs_per_step = T * T * NT * N
+
+    def step(j):
+        out, vel = tile_args[my_tiles[j]]
+        k.migrate_tile(tb, out, vel)
+
+    for j in range(args.warmup):
+        step(j)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for j in range(args.warmup, args.warmup + args.steps):
+            step(j)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * pairs_per_step / (ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- roofline of the migration kernel (one launch per step; the per-step
+    # table kernel is ~1e-5 of the step)
+    per_launch_s = ms / 1e3 / args.steps
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    mufu_peak = 148 * 16 * sm_mhz * 1e6          # MUFU ops/s, derived: 148 SMs x 16/clk x median SM clock
+    achieved_mufu = pairs_per_step * MUFU_PER_PAIR / per_launch_s
+    elem = amps.element_size()
+    alg_bytes = N * NS * elem + N * 6 * 8 + T * T * NT * (8 + 8 + 4 + 4) + T * T * NT * 8
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    roofline = {
+        "bound": "sfu", "unit": "Gop/s", "achieved": achieved_mufu / 1e9, "peak": mufu_peak / 1e9,
+        "frac": achieved_mufu / mufu_peak,
+        "peak_source": "derived: 148 SMs x 16 MUFU/clk x median SM clock under load (no measured SFU peak)",
+        "per_pair": f"{FLOP_PER_PAIR} FP32 FLOP + {MUFU_PER_PAIR} MUFU (straight-ray DSR + AA + weights)",
+        "fp32": {"achieved_tflops": pairs_per_step * FLOP_PER_PAIR / per_launch_s / 1e12,
+                 "peak_tflops": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12},
+        "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
+                "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes},
+        "traffic": None,
+    }
+
+    # ---- end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_amps = torch.empty(amps.shape, dtype=amps.dtype, pin_memory=True)
+        h_amps.copy_(amps)
+        amps_np = h_amps.view(torch.int16).numpy().view(np.uint16) if tdtype == torch.bfloat16 else h_amps.numpy()
+
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+        htb = TraceBlock(amplitudes=amps_np, offset=pinned(offset.cpu().numpy()), sample_rate_ms=DT_MS,
+                         start_time_ms=0.0, **{kk: pinned(v.cpu().numpy()) for kk, v in geo.items()})
+        h_img = torch.zeros((T, T, NT), dtype=torch.float64, pin_memory=True).numpy()
+        h_fold = torch.zeros((T, T, NT), dtype=torch.int32, pin_memory=True).numpy()
+        h_tiles = {}
+        for tl in set(my_tiles):
+            ix0, ix1, iy0, iy1 = tl
+            h_tiles[tl] = (OutputTile(image=h_img, fold=h_fold, x_axis=sv.x_axis[ix0:ix1], y_axis=sv.y_axis[iy0:iy1],
+                                      t_axis_ms=sv.t_axis_ms),
+                           VelocitySlice(vrms=pinned(sv.velocity(ix0, ix1, iy0, iy1)), is_1d=False))
+        ke = CudaKernel(trace_dtype="auto")
+        ke.initialize(cfg)
+        ke.migrate_tile(htb, *h_tiles[my_tiles[0]])   # warm the staging buffers
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for j in range(args.e2e_steps):
+            ke.migrate_tile(htb, *h_tiles[my_tiles[j % len(my_tiles)]])
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = amps_np.nbytes + sum(htb.__dict__[kk].nbytes for kk in geo) + T * T * NT * (8 + 8 + 4) + \
+            3 * T * 8 + NT * 8
+        d2h = T * T * NT * (8 + 4)
+        e2e = {"value": world * args.e2e_steps * pairs_per_step / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "steps": args.e2e_steps, "timer": "perf_counter around synchronous migrate_tile calls"}
+        ke.cleanup()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        oracle.build()
+        n_tr = 1 << 18
+        amps_host = amps[:n_tr].float().cpu().numpy()
+        rate, pairs, dt = cpu_sample(sv, cfg, tiles[0], n_tr, 4, 4, amps_host)
+        cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"4x4 pillars x {NT} samples x {n_tr} traces ({pairs:.3g} pairs, {dt:.1f} s), "
+                         "FP64 C port of the reference semantics, OpenMP on all host threads"}
+
+    k.cleanup()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": "case-2 production tile: 1,048,576 traces x 1500 samples @2 ms, "
+                                   "3.2 km patch, 3-D v_rms, AA on, 5 km aperture; one step = "
+                                   f"{T}x{T}x{NT} output tile (pillars x samples)",
+                       "traces": N, "tile": [T, T, NT], "grid": [GRID, GRID, NT], "traveltime": "straight_ray",
+                       "trace_dtype": args.dtype, "accumulate": "fp32 compensated -> f64 image",
+                       "l2": "inputs larger than L2 (trace panel > 126 MB), no flush",
+                       "parallelism": f"replicas x{world} (disjoint tiles)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 2 * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        main_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,154 @@
+/*
+ * pstm_cuda.h -- C ABI of the B200 (sm_100a) Kirchhoff PSTM backend.
+ *
+ * This library is the CUDA counterpart of the reference `pstm` package's
+ * kernel backends (Numba CPU, Metal).  Each entry point below names the
+ * reference interface it replaces (paths relative to the reference project).
+ * All descriptors carry plain pointers and sizes; no C++ or framework types
+ * cross this boundary.  Every function returns a pstm_status; 0 is success and
+ * a nonzero status leaves a message in pstm_cuda_last_error().
+ *
+ * Pointer spaces: the *_dev entry points take DEVICE pointers (cudaMalloc'd or
+ * any device-accessible memory) and run asynchronously on the given stream;
+ * the *_host entry points take HOST pointers, stage them through buffers the
+ * context owns and return after the result has been copied back.
+ *
+ * Accumulation semantics follow the reference Numba backend
+ * (pstm/kernels/numba_cpu_optimized.py:147-231): image is accumulated with
+ * "+=", and fold receives, for every pillar, the number of traces whose
+ * midpoint lies within max_aperture_m, added to every output sample of that
+ * pillar when fold is 3-D (nx, ny, nt) or once when it is 2-D (nx, ny).
+ */
+#ifndef PSTM_CUDA_H
+#define PSTM_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSTM_CUDA_ABI_VERSION 1
+
+typedef enum {
+    PSTM_OK = 0,
+    PSTM_ERR_INVALID_ARGUMENT = 1,  /* reference: ValueError */
+    PSTM_ERR_CUDA = 2,              /* reference: RuntimeError from the device */
+    PSTM_ERR_OUT_OF_MEMORY = 3,
+    PSTM_ERR_NOT_INITIALIZED = 4,   /* reference: RuntimeError("Kernel not initialized") */
+    PSTM_ERR_UNSUPPORTED = 5,
+    PSTM_ERR_TIMEOUT = 6,           /* a bounded device-side wait gave up */
+    PSTM_ERR_INJECTED = 7           /* host-side fault injection (PSTM_CUDA_INJECT_FAULT) */
+} pstm_status;
+
+typedef enum { PSTM_AMP_F32 = 0, PSTM_AMP_BF16 = 1, PSTM_AMP_F16 = 2 } pstm_amp_dtype;
+typedef enum { PSTM_IMAGE_F64 = 0, PSTM_IMAGE_F32 = 1 } pstm_image_dtype;
+
+/* Traveltime kinds.  Reference: executor dispatch pstm/pipeline/executor.py:1691-1745
+ * (migrate_tile / migrate_tile_curved_ray / migrate_tile_vti). */
+typedef enum {
+    PSTM_TT_STRAIGHT = 0,    /* DSR, numba_cpu_optimized.py:192-194 */
+    PSTM_TT_CURVED = 1,      /* V(z)=v0+kz, pstm_curved_ray.metal:50-96 */
+    PSTM_TT_VTI = 2,         /* eta moveout, pstm_anisotropic_vti.metal:103-148 */
+    PSTM_TT_CURVED_VTI = 3   /* curved leg with the VTI quartic correction (no reference formula) */
+} pstm_traveltime;
+
+/* Trace panel + geometry.  Reference carrier: TraceBlock, pstm/kernels/base.py:27-116. */
+typedef struct {
+    const void *amplitudes;       /* (n_traces, amp_row_stride) of amp_dtype */
+    int32_t amp_dtype;            /* pstm_amp_dtype */
+    int32_t n_samples;            /* samples per trace (>= 2) */
+    int64_t n_traces;
+    int64_t amp_row_stride;       /* elements between trace rows (>= n_samples) */
+    const double *source_x, *source_y;
+    const double *receiver_x, *receiver_y;
+    const double *midpoint_x, *midpoint_y;
+    const double *weights;        /* nullable: all ones */
+    double sample_rate_ms;
+    double start_time_ms;
+} pstm_traces_desc;
+
+/* Output tile.  Reference carrier: OutputTile, pstm/kernels/base.py:119-177. */
+typedef struct {
+    void *image;                  /* (nx, ny, nt), accumulated with += */
+    int32_t image_dtype;          /* pstm_image_dtype */
+    int32_t fold_is_3d;           /* 1: fold is (nx, ny, nt); 0: (nx, ny) */
+    int32_t *fold;                /* nullable */
+    int32_t nx, ny, nt;
+    const double *x_axis;         /* (nx) */
+    const double *y_axis;         /* (ny) */
+    const double *x_grid;         /* nullable (nx*ny): rotated-grid coordinates */
+    const double *y_grid;         /* nullable (nx*ny) */
+    const double *t_axis_ms;      /* (nt) output times */
+} pstm_output_desc;
+
+/* RMS velocity.  Reference carrier: VelocitySlice, pstm/kernels/base.py:180-194. */
+typedef struct {
+    const double *vrms;           /* (nt) or (nx, ny, nt) */
+    int32_t is_3d;
+    int32_t reserved;
+} pstm_velocity_desc;
+
+/* Kernel parameters.  Reference carrier: KernelConfig, pstm/kernels/base.py:197-265. */
+typedef struct {
+    double max_aperture_m;
+    double min_aperture_m;
+    double max_dip_degrees;
+    double taper_fraction;
+    int32_t apply_spreading;
+    int32_t apply_obliquity;
+    int32_t aa_enabled;           /* triangle AA weight, pstm_migration.metal:95-132 */
+    int32_t traveltime;           /* pstm_traveltime */
+    double aa_dominant_freq;      /* Hz; reference default 30 (metal_compiled.py:706) */
+    double grid_dx, grid_dy;      /* bin spacing used by the AA weight */
+    double curved_v0, curved_k;   /* V(z) = v0 + k z */
+    const double *eta;            /* nullable: eta_constant; else (nt) or (nx, ny, nt) */
+    int32_t eta_is_3d;
+    int32_t compensated;          /* 1: compensated (TwoSum) FP32 accumulation */
+    double eta_constant;
+} pstm_params;
+
+/* Library / ABI version (no reference counterpart: a binding sanity check). */
+int32_t pstm_cuda_abi_version(void);
+
+/* Create a context on a CUDA device.  Replaces the backend constructor +
+ * initialize(): MigrationKernel.initialize, pstm/kernels/base.py:302;
+ * OptimizedNumbaKernel.initialize, numba_cpu_optimized.py:498-543. */
+int32_t pstm_cuda_create(int32_t device, void **ctx_out);
+
+/* Release a context and every buffer it owns.  Replaces
+ * MigrationKernel.cleanup, pstm/kernels/base.py:317. */
+void pstm_cuda_destroy(void *ctx);
+
+/* Migrate one tile, device pointers, asynchronous on `stream` (a
+ * cudaStream_t; NULL = the context's stream).  Replaces
+ * MigrationKernel.migrate_tile, base.py:305-313;
+ * OptimizedNumbaKernel.migrate_tile, numba_cpu_optimized.py:545-626;
+ * CompiledMetalKernel.migrate_tile[_curved_ray/_vti], metal_compiled.py:567,1275,1456. */
+int32_t pstm_cuda_migrate_tile_dev(void *ctx, const pstm_traces_desc *traces,
+                                   const pstm_output_desc *output,
+                                   const pstm_velocity_desc *velocity,
+                                   const pstm_params *params, void *stream);
+
+/* Same, host pointers: inputs are copied to the device, the tile is migrated
+ * and image/fold are copied back and accumulated (+=) into the host arrays.
+ * Synchronous, like the reference backends.  Native precedent: the pybind11
+ * migrate_tile binding, pstm/metal/src/bindings.cpp:48-62. */
+int32_t pstm_cuda_migrate_tile_host(void *ctx, const pstm_traces_desc *traces,
+                                    const pstm_output_desc *output,
+                                    const pstm_velocity_desc *velocity,
+                                    const pstm_params *params);
+
+/* Wait for all work queued on the context's stream.  Replaces
+ * MigrationKernel.synchronize, pstm/kernels/base.py:315. */
+int32_t pstm_cuda_synchronize(void *ctx);
+
+/* Message of the last failing call on this context (or of the last failing
+ * pstm_cuda_create when ctx is NULL).  Reference: the RuntimeError text the
+ * Metal backend raises, metal_compiled.py:763-764. */
+const char *pstm_cuda_last_error(void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSTM_CUDA_H */

@@ -1,0 +1,121 @@
+"""ctypes binding of ``libpstm_cuda.so`` (the C ABI in ``include/pstm_cuda.h``).
+
+The structures below mirror the header field for field.  Loading fails loudly
+when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpstm_cuda.so")
+
+ABI_VERSION = 1
+
+# pstm_status
+OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_INITIALIZED, \
+    ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_INJECTED = range(8)
+STATUS_NAMES = {
+    OK: "PSTM_OK", ERR_INVALID_ARGUMENT: "PSTM_ERR_INVALID_ARGUMENT", ERR_CUDA: "PSTM_ERR_CUDA",
+    ERR_OUT_OF_MEMORY: "PSTM_ERR_OUT_OF_MEMORY", ERR_NOT_INITIALIZED: "PSTM_ERR_NOT_INITIALIZED",
+    ERR_UNSUPPORTED: "PSTM_ERR_UNSUPPORTED", ERR_TIMEOUT: "PSTM_ERR_TIMEOUT",
+    ERR_INJECTED: "PSTM_ERR_INJECTED",
+}
+
+AMP_F32, AMP_BF16, AMP_F16 = 0, 1, 2
+IMAGE_F64, IMAGE_F32 = 0, 1
+TT_STRAIGHT, TT_CURVED, TT_VTI, TT_CURVED_VTI = 0, 1, 2, 3
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+
+class TracesDesc(ctypes.Structure):
+    _fields_ = [
+        ("amplitudes", _vp), ("amp_dtype", ctypes.c_int32), ("n_samples", ctypes.c_int32),
+        ("n_traces", ctypes.c_int64), ("amp_row_stride", ctypes.c_int64),
+        ("source_x", _vp), ("source_y", _vp), ("receiver_x", _vp), ("receiver_y", _vp),
+        ("midpoint_x", _vp), ("midpoint_y", _vp), ("weights", _vp),
+        ("sample_rate_ms", ctypes.c_double), ("start_time_ms", ctypes.c_double),
+    ]
+
+
+class OutputDesc(ctypes.Structure):
+    _fields_ = [
+        ("image", _vp), ("image_dtype", ctypes.c_int32), ("fold_is_3d", ctypes.c_int32),
+        ("fold", _vp), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nt", ctypes.c_int32),
+        ("x_axis", _vp), ("y_axis", _vp), ("x_grid", _vp), ("y_grid", _vp), ("t_axis_ms", _vp),
+    ]
+
+
+class VelocityDesc(ctypes.Structure):
+    _fields_ = [("vrms", _vp), ("is_3d", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("max_aperture_m", ctypes.c_double), ("min_aperture_m", ctypes.c_double),
+        ("max_dip_degrees", ctypes.c_double), ("taper_fraction", ctypes.c_double),
+        ("apply_spreading", ctypes.c_int32), ("apply_obliquity", ctypes.c_int32),
+        ("aa_enabled", ctypes.c_int32), ("traveltime", ctypes.c_int32),
+        ("aa_dominant_freq", ctypes.c_double), ("grid_dx", ctypes.c_double),
+        ("grid_dy", ctypes.c_double), ("curved_v0", ctypes.c_double), ("curved_k", ctypes.c_double),
+        ("eta", _vp), ("eta_is_3d", ctypes.c_int32), ("compensated", ctypes.c_int32),
+        ("eta_constant", ctypes.c_double),
+    ]
+
+
+# name -> (restype, argtypes); the exported surface of include/pstm_cuda.h
+SIGNATURES = {
+    "pstm_cuda_abi_version": (ctypes.c_int32, []),
+    "pstm_cuda_create": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "pstm_cuda_destroy": (None, [_vp]),
+    "pstm_cuda_migrate_tile_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
+                                                    ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
+    "pstm_cuda_migrate_tile_host": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
+                                                     ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
+    "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
+    "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
+}
+
+_lib = None
+
+
+class PstmCudaError(RuntimeError):
+    """A nonzero pstm_status, carrying the code and the library's message."""
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+
+
+def load(path: str | None = None):
+    """Load the library (once) and bind every declared entry point."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m pstm_b200.build` (there is no CPU fallback)")
+    L = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    if L.pstm_cuda_abi_version() != ABI_VERSION:
+        raise RuntimeError("libpstm_cuda.so ABI version mismatch; rebuild")
+    if path is None:
+        _lib = L
+    return L
+
+
+def check(rc: int, ctx=None, lib=None) -> None:
+    if rc != OK:
+        L = lib or load()
+        msg = L.pstm_cuda_last_error(ctx)
+        msg = msg.decode() if msg else ""
+        if rc == ERR_INVALID_ARGUMENT:
+            raise ValueError(f"PSTM_ERR_INVALID_ARGUMENT: {msg}")
+        raise PstmCudaError(rc, msg)

@@ -1,0 +1,408 @@
+// capi.cu -- the C ABI declared in include/pstm_cuda.h: contexts, argument
+// validation, launch-parameter derivation and the host-pointer staging path.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pstm_cuda.h"
+#include "kparams.h"
+#include "migrate_dispatch.cuh"
+
+namespace pstm {
+template <int TT>
+cudaError_t launch_migrate_tt(const KParams &, int, bool, bool, const TileShape &, dim3, cudaStream_t);
+__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab);
+}  // namespace pstm
+
+using namespace pstm;
+
+namespace {
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevBuf ttab;
+    // staging for the host-pointer path
+    DevBuf amps, geo[7], xa, ya, xg, yg, ta, vel, eta, image, fold;
+    TileShape shape{2, 8, 64};
+};
+
+thread_local std::string g_create_err;
+
+struct Status {
+    int32_t code;
+};
+
+int32_t fail(Ctx *c, int32_t code, const std::string &msg) {
+    if (c) c->err = msg;
+    else g_create_err = msg;
+    return code;
+}
+
+int32_t cuda_fail(Ctx *c, cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(c, e == cudaErrorMemoryAllocation ? PSTM_ERR_OUT_OF_MEMORY : PSTM_ERR_CUDA, m);
+}
+
+bool injected(const char *site) {
+    const char *v = std::getenv("PSTM_CUDA_INJECT_FAULT");
+    if (!v || !*v) return false;
+    return std::strcmp(v, site) == 0 || std::strcmp(v, "all") == 0;
+}
+
+cudaError_t ensure(DevBuf &b, size_t bytes) {
+    if (bytes <= b.bytes && b.ptr) return cudaSuccess;
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e == cudaSuccess) b.bytes = want;
+    return e;
+}
+
+void release(DevBuf &b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+size_t amp_elem_bytes(int32_t dt) { return dt == PSTM_AMP_F32 ? 4 : 2; }
+
+// Largest double B such that the correctly rounded sqrt(B) <= a, i.e. the
+// FP64 predicate "sqrt(d2) > a" used by the reference equals "d2 > B".
+double sqrt_threshold(double a) {
+    double b = a * a;
+    while (std::sqrt(b) > a) b = std::nextafter(b, 0.0);
+    while (std::sqrt(std::nextafter(b, INFINITY)) <= a) b = std::nextafter(b, INFINITY);
+    return b;
+}
+
+int32_t validate(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
+                 const pstm_velocity_desc *vel, const pstm_params *prm) {
+    if (!tr || !out || !vel || !prm) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null descriptor");
+    if (tr->n_traces < 0) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "n_traces < 0");
+    if (tr->n_samples < 2) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "n_samples must be >= 2");
+    if (tr->amp_dtype < PSTM_AMP_F32 || tr->amp_dtype > PSTM_AMP_F16)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown amplitude dtype");
+    if (tr->amp_row_stride < tr->n_samples)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "amp_row_stride < n_samples");
+    if (tr->n_traces > 0 && (!tr->amplitudes || !tr->source_x || !tr->source_y || !tr->receiver_x ||
+                             !tr->receiver_y || !tr->midpoint_x || !tr->midpoint_y))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null trace array");
+    if (!(tr->sample_rate_ms > 0.0)) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "sample_rate_ms must be > 0");
+    if (out->nx <= 0 || out->ny <= 0 || out->nt <= 0)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "empty output tile");
+    if (!out->image) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null image");
+    if (out->image_dtype != PSTM_IMAGE_F64 && out->image_dtype != PSTM_IMAGE_F32)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown image dtype");
+    if (!out->t_axis_ms) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null t axis");
+    if ((!out->x_grid || !out->y_grid) && (!out->x_axis || !out->y_axis))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "need x/y axes or x/y grids");
+    if ((out->x_grid == nullptr) != (out->y_grid == nullptr))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "x_grid and y_grid must be given together");
+    if (!vel->vrms) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null velocity");
+    if (prm->traveltime < PSTM_TT_STRAIGHT || prm->traveltime > PSTM_TT_CURVED_VTI)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown traveltime kind");
+    if (!(prm->max_aperture_m >= 0.0) || !(prm->taper_fraction >= 0.0) || !(prm->taper_fraction <= 1.0))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "bad aperture/taper parameters");
+    if ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) && !(prm->curved_v0 > 0.0))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "curved_v0 must be > 0");
+    return PSTM_OK;
+}
+
+KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
+                    const pstm_params *prm, const TileShape &sh) {
+    KParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.amps = tr->amplitudes;
+    P.amp_stride = tr->amp_row_stride;
+    P.n_traces = tr->n_traces;
+    P.ns = tr->n_samples;
+    P.sx = tr->source_x; P.sy = tr->source_y;
+    P.rx = tr->receiver_x; P.ry = tr->receiver_y;
+    P.mx = tr->midpoint_x; P.my = tr->midpoint_y;
+    P.w = tr->weights;
+    P.dt_s = tr->sample_rate_ms / 1000.0;
+    P.tstart_s = tr->start_time_ms / 1000.0;
+    P.s_scale = (float)(1.0 / P.dt_s);
+    P.s_offset = (float)(-P.tstart_s / P.dt_s);
+    const float g = 1e-2f;   // guard band in samples around the FP64 decision boundaries
+    const float smax = (float)(tr->n_samples - 1);
+    P.s_guard_lo = g;
+    P.s_guard_hi = smax - g;
+    P.s_rej_lo = -g;
+    P.s_rej_hi = smax + g;
+    P.s_max_clamp = std::nextafter(smax, 0.0f);
+
+    P.image = out->image;
+    P.fold = out->fold;
+    P.image_f32 = out->image_dtype == PSTM_IMAGE_F32;
+    P.fold3d = out->fold_is_3d;
+    P.nx = out->nx; P.ny = out->ny; P.nt = out->nt;
+    P.xa = out->x_axis; P.ya = out->y_axis;
+    P.xg = out->x_grid; P.yg = out->y_grid;
+    P.ta = out->t_axis_ms;
+
+    P.vrms = vel->vrms;
+    P.vel3d = vel->is_3d;
+    P.eta = prm->eta;
+    P.eta3d = prm->eta ? prm->eta_is_3d : 0;
+    P.eta_const = prm->eta_constant;
+
+    P.max_ap = prm->max_aperture_m;
+    P.min_ap = prm->min_aperture_m;
+    P.tan_dip = std::tan(prm->max_dip_degrees * M_PI / 180.0);
+    P.taper = prm->taper_fraction;
+    P.fold_d2_max = sqrt_threshold(prm->max_aperture_m);
+    P.ap_max_f = (float)prm->max_aperture_m;
+    P.taper_f = (float)prm->taper_fraction;
+    P.spreading = prm->apply_spreading ? 1 : 0;
+    P.obliquity = prm->apply_obliquity ? 1 : 0;
+    P.aa = prm->aa_enabled ? 1 : 0;
+    const double gmax = prm->grid_dx > prm->grid_dy ? prm->grid_dx : prm->grid_dy;
+    P.aa_cA = (float)(4.0 * gmax * prm->aa_dominant_freq);
+    P.aa_cB = (float)(prm->aa_dominant_freq / 500.0);
+    P.cr_v0 = prm->curved_v0;
+    P.cr_k = prm->curved_k;
+    P.cr_v0f = (float)prm->curved_v0;
+    P.cr_kf = (float)prm->curved_k;
+    P.cr_k_zero = std::fabs(prm->curved_k) < 1e-10 ? 1 : 0;
+    P.cr_inv_k_ln2 = P.cr_k_zero ? 0.f : (float)(M_LN2 / prm->curved_k);
+    P.compensated = prm->compensated ? 1 : 0;
+
+    // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)
+    int py = sh.PB, px = 1;
+    while (py > 1 && py > out->ny) { py /= 2; px *= 2; }
+    if (py == sh.PB && sh.PB >= 4) { py = sh.PB / 2; px = 2; }
+    P.px = px;
+    P.py = py;
+    P.n_pblk_y = (out->ny + py - 1) / py;
+    return P;
+}
+
+int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
+                const pstm_velocity_desc *vel, const pstm_params *prm, cudaStream_t st) {
+    int32_t rc = validate(c, tr, out, vel, prm);
+    if (rc) return rc;
+    if (injected("migrate")) return fail(c, PSTM_ERR_INJECTED, "injected fault: migrate");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    KParams P = make_params(tr, out, vel, prm, c->shape);
+    if (tr->n_traces == 0) return PSTM_OK;   // nothing to add: image += 0, fold += 0
+
+    const bool per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
+    const int64_t n_p = per_pillar ? (int64_t)out->nx * out->ny : 1;
+    e = ensure(c->ttab, (size_t)n_p * out->nt * sizeof(float4));
+    if (e != cudaSuccess) return cuda_fail(c, e, "allocating the time table");
+    float4 *tab = reinterpret_cast<float4 *>(c->ttab.ptr);
+    {
+        const int64_t n = n_p * out->nt;
+        int blocks = (int)((n + 255) / 256);
+        if (blocks > 148 * 32) blocks = 148 * 32;
+        prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(c, e, "prep_time_table launch");
+    }
+    P.ttab = tab;
+
+    const TileShape &sh = c->shape;
+    const int n_pblk_x = (out->nx + P.px - 1) / P.px;
+    const int64_t nblk_p = (int64_t)n_pblk_x * P.n_pblk_y;
+    const int nblk_t = (out->nt + kThreads * sh.R - 1) / (kThreads * sh.R);
+    if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(c, PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
+    dim3 grid((unsigned)nblk_p, (unsigned)nblk_t);
+    switch (prm->traveltime) {
+    case PSTM_TT_STRAIGHT: e = launch_migrate_tt<TT_STRAIGHT>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
+    case PSTM_TT_CURVED: e = launch_migrate_tt<TT_CURVED>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
+    case PSTM_TT_VTI: e = launch_migrate_tt<TT_VTI>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
+    default: e = launch_migrate_tt<TT_CURVED_VTI>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "migrate kernel launch");
+    return PSTM_OK;
+}
+
+template <typename T>
+cudaError_t stage(DevBuf &b, const T *src, size_t count, cudaStream_t st, const T **dst) {
+    if (!src) {
+        *dst = nullptr;
+        return cudaSuccess;
+    }
+    cudaError_t e = ensure(b, count * sizeof(T));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(b.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice, st);
+    *dst = reinterpret_cast<const T *>(b.ptr);
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pstm_cuda_abi_version(void) { return PSTM_CUDA_ABI_VERSION; }
+
+int32_t pstm_cuda_create(int32_t device, void **ctx_out) {
+    if (!ctx_out) return fail(nullptr, PSTM_ERR_INVALID_ARGUMENT, "ctx_out is null");
+    *ctx_out = nullptr;
+    if (injected("create")) return fail(nullptr, PSTM_ERR_INJECTED, "injected fault: create");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(nullptr, PSTM_ERR_INVALID_ARGUMENT, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    Ctx *c = new Ctx();
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(nullptr, e, "cudaStreamCreate");
+    }
+    const char *shape = std::getenv("PSTM_CUDA_TILE");   // "R,PB,C" override
+    if (shape) {
+        int r, pb, cc;
+        if (std::sscanf(shape, "%d,%d,%d", &r, &pb, &cc) == 3) c->shape = TileShape{r, pb, cc};
+    }
+    *ctx_out = c;
+    return PSTM_OK;
+}
+
+void pstm_cuda_destroy(void *ctx) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    release(c->ttab);
+    release(c->amps);
+    for (auto &g : c->geo) release(g);
+    release(c->xa); release(c->ya); release(c->xg); release(c->yg); release(c->ta);
+    release(c->vel); release(c->eta); release(c->image); release(c->fold);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int32_t pstm_cuda_migrate_tile_dev(void *ctx, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                   const pstm_velocity_desc *velocity, const pstm_params *params, void *stream) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return fail(nullptr, PSTM_ERR_NOT_INITIALIZED, "Kernel not initialized");
+    cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->stream;
+    return run_dev(c, traces, output, velocity, params, st);
+}
+
+static int32_t migrate_host_impl(Ctx *c, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                 const pstm_velocity_desc *velocity, const pstm_params *params);
+
+int32_t pstm_cuda_migrate_tile_host(void *ctx, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                    const pstm_velocity_desc *velocity, const pstm_params *params) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return fail(nullptr, PSTM_ERR_NOT_INITIALIZED, "Kernel not initialized");
+    int32_t rc = migrate_host_impl(c, traces, output, velocity, params);
+    // On failure, drain the stream so no queued copy outlives the caller's buffers.
+    if (rc != PSTM_OK && c->stream) cudaStreamSynchronize(c->stream);
+    return rc;
+}
+
+static int32_t migrate_host_impl(Ctx *c, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                 const pstm_velocity_desc *velocity, const pstm_params *params) {
+    int32_t rc = validate(c, traces, output, velocity, params);
+    if (rc) return rc;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    cudaStream_t st = c->stream;
+    const int64_t N = traces->n_traces;
+    const int nx = output->nx, ny = output->ny, nt = output->nt;
+    const size_t npix = (size_t)nx * ny * nt;
+
+    pstm_traces_desc dt = *traces;
+    pstm_output_desc dout = *output;
+    pstm_velocity_desc dv = *velocity;
+    pstm_params dp = *params;
+    const size_t eb = amp_elem_bytes(traces->amp_dtype);
+    // amplitudes: packed to n_samples per row on the device
+    if (N > 0) {
+        e = ensure(c->amps, (size_t)N * traces->n_samples * eb);
+        if (e != cudaSuccess) return cuda_fail(c, e, "staging amplitudes");
+        e = cudaMemcpy2DAsync(c->amps.ptr, traces->n_samples * eb, traces->amplitudes,
+                              traces->amp_row_stride * eb, traces->n_samples * eb, (size_t)N,
+                              cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(c, e, "copying amplitudes");
+        dt.amplitudes = c->amps.ptr;
+        dt.amp_row_stride = traces->n_samples;
+    }
+    const double *src_geo[7] = {traces->source_x, traces->source_y, traces->receiver_x, traces->receiver_y,
+                                traces->midpoint_x, traces->midpoint_y, traces->weights};
+    const double *dst_geo[7];
+    for (int i = 0; i < 7; ++i) {
+        e = stage(c->geo[i], N > 0 ? src_geo[i] : nullptr, (size_t)N, st, &dst_geo[i]);
+        if (e != cudaSuccess) return cuda_fail(c, e, "copying geometry");
+    }
+    dt.source_x = dst_geo[0]; dt.source_y = dst_geo[1];
+    dt.receiver_x = dst_geo[2]; dt.receiver_y = dst_geo[3];
+    dt.midpoint_x = dst_geo[4]; dt.midpoint_y = dst_geo[5];
+    dt.weights = dst_geo[6];
+
+    if ((e = stage(c->xa, output->x_axis, (size_t)nx, st, &dout.x_axis)) != cudaSuccess ||
+        (e = stage(c->ya, output->y_axis, (size_t)ny, st, &dout.y_axis)) != cudaSuccess ||
+        (e = stage(c->xg, output->x_grid, (size_t)nx * ny, st, &dout.x_grid)) != cudaSuccess ||
+        (e = stage(c->yg, output->y_grid, (size_t)nx * ny, st, &dout.y_grid)) != cudaSuccess ||
+        (e = stage(c->ta, output->t_axis_ms, (size_t)nt, st, &dout.t_axis_ms)) != cudaSuccess)
+        return cuda_fail(c, e, "copying output axes");
+    const size_t nvel = velocity->is_3d ? npix : (size_t)nt;
+    if ((e = stage(c->vel, velocity->vrms, nvel, st, &dv.vrms)) != cudaSuccess)
+        return cuda_fail(c, e, "copying velocity");
+    if (params->eta) {
+        const size_t neta = params->eta_is_3d ? npix : (size_t)nt;
+        if ((e = stage(c->eta, params->eta, neta, st, &dp.eta)) != cudaSuccess)
+            return cuda_fail(c, e, "copying eta");
+    }
+    const size_t img_bytes = npix * (output->image_dtype == PSTM_IMAGE_F32 ? 4 : 8);
+    if ((e = ensure(c->image, img_bytes)) != cudaSuccess) return cuda_fail(c, e, "staging image");
+    if ((e = cudaMemcpyAsync(c->image.ptr, output->image, img_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(c, e, "copying image");
+    dout.image = c->image.ptr;
+    const size_t fold_bytes = (output->fold_is_3d ? npix : (size_t)nx * ny) * sizeof(int32_t);
+    if (output->fold) {
+        if ((e = ensure(c->fold, fold_bytes)) != cudaSuccess) return cuda_fail(c, e, "staging fold");
+        if ((e = cudaMemcpyAsync(c->fold.ptr, output->fold, fold_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return cuda_fail(c, e, "copying fold");
+        dout.fold = reinterpret_cast<int32_t *>(c->fold.ptr);
+    }
+    rc = run_dev(c, &dt, &dout, &dv, &dp, st);
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(output->image, c->image.ptr, img_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(c, e, "reading image back");
+    if (output->fold &&
+        (e = cudaMemcpyAsync(output->fold, c->fold.ptr, fold_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(c, e, "reading fold back");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(c, e, "migrate_tile");
+    return PSTM_OK;
+}
+
+int32_t pstm_cuda_synchronize(void *ctx) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return fail(nullptr, PSTM_ERR_NOT_INITIALIZED, "Kernel not initialized");
+    if (injected("sync")) return fail(c, PSTM_ERR_INJECTED, "injected fault: sync");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "synchronize");
+    return PSTM_OK;
+}
+
+const char *pstm_cuda_last_error(void *ctx) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    return c ? c->err.c_str() : g_create_err.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// kparams.h -- launch parameters shared by the host side (capi.cu) and the
+// migration kernels.  Plain C++ struct passed by value to every launch.
+#pragma once
+#include <stdint.h>
+
+namespace pstm {
+
+enum AmpKind { AMP_F32 = 0, AMP_BF16 = 1, AMP_F16 = 2 };
+enum TTKind { TT_STRAIGHT = 0, TT_CURVED = 1, TT_VTI = 2, TT_CURVED_VTI = 3 };
+
+struct KParams {
+    // ---- traces ----
+    const void *amps;
+    int64_t amp_stride;          // elements between rows
+    int64_t n_traces;
+    int32_t ns;                  // samples per trace
+    int32_t pad0;
+    const double *sx, *sy, *rx, *ry, *mx, *my, *w;   // w nullable
+    double dt_s, tstart_s;       // input sampling (seconds)
+    float s_scale, s_offset;     // sample index s = T * s_scale + s_offset
+    float s_guard_lo, s_guard_hi;  // fast-path accept window for s
+    float s_rej_lo, s_rej_hi;    // outside [s_rej_lo, s_rej_hi] the pair is rejected
+    float s_max_clamp;           // largest s allowed for the interpolation read
+    int32_t pad1;
+
+    // ---- output ----
+    void *image;
+    int32_t *fold;
+    int32_t image_f32;           // 0: f64 image, 1: f32 image
+    int32_t fold3d;
+    int32_t nx, ny, nt;
+    int32_t px, py;              // pillar patch of one CTA (px * py pillars)
+    int32_t n_pblk_y;            // number of patches along y
+    const double *xa, *ya, *xg, *yg, *ta;   // xg/yg nullable
+
+    // ---- velocity / per-time tables ----
+    const double *vrms;          // (nt) or (nx*ny*nt), FP64 (exact paths)
+    int32_t vel3d;
+    int32_t eta3d;
+    const float4 *ttab;          // per (pillar|0, t): {iv2, ap, eta, 1/v}
+    const double *eta;           // nullable (FP64, exact paths)
+    double eta_const;
+
+    // ---- parameters ----
+    double max_ap, min_ap, tan_dip, taper;
+    double fold_d2_max;          // largest d^2 with RN(sqrt(d^2)) <= max_ap
+    float ap_max_f;              // (float)max_ap
+    float taper_f;               // taper fraction
+    int32_t spreading, obliquity;
+    int32_t aa;
+    float aa_cA, aa_cB;          // 4*max(dx,dy)*f_dom, f_dom/500
+    double cr_v0, cr_k;
+    float cr_v0f, cr_kf, cr_inv_k_ln2;   // inv_k * ln2 (log2 based)
+    int32_t cr_k_zero;           // |k| < 1e-10: straight-ray fallback with v0
+    int32_t compensated;
+    int32_t pad2;
+};
+
+}  // namespace pstm

@@ -1,0 +1,334 @@
+"""CUDA backend implementing the reference ``MigrationKernel`` protocol.
+
+Drop-in for the reference's kernel backends (``pstm/kernels/base.py:290-318``):
+``name``, ``capabilities``, ``initialize``, ``migrate_tile``, ``synchronize``,
+``cleanup``, plus the optional methods the reference executor discovers with
+``hasattr`` (``pstm/pipeline/executor.py:1710-1745``):
+``migrate_tile_curved_ray`` and ``migrate_tile_vti``.  ``migrate_tile_curved_vti``
+is an extension with no reference counterpart.
+
+Arguments are duck-typed, so the reference's own ``TraceBlock``/``OutputTile``/
+``VelocitySlice``/``KernelConfig`` objects work as well as this package's
+mirrors.  NumPy arrays go through the host-pointer C entry point (copies in,
+kernel, copies out); CUDA ``torch`` tensors go through the device-pointer entry
+point without copies.
+
+Semantics follow the reference Numba backend
+(``pstm/kernels/numba_cpu_optimized.py:545-626``): the image and fold are
+accumulated in place (``+=``), a 1-D velocity shorter or longer than the
+output time axis is interpolated onto it with ``np.interp`` (:569-578), and
+calling ``migrate_tile`` before ``initialize`` raises
+``RuntimeError("Kernel not initialized")`` (:555-556).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import time
+
+import numpy as np
+
+from . import _native as nat
+from .base import KernelCapability, KernelMetrics
+
+_TT_BY_TYPE = {
+    "straight_ray": nat.TT_STRAIGHT,
+    "curved_ray": nat.TT_CURVED,
+    "anisotropic_vti": nat.TT_VTI,
+    "curved_vti": nat.TT_CURVED_VTI,
+}
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and hasattr(x, "data_ptr") and bool(x.is_cuda)
+
+
+def float32_to_bf16_bits(a: np.ndarray) -> np.ndarray:
+    """Round-to-nearest-even FP32 -> BF16, returned as uint16 bit patterns."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    rounding = ((u >> 16) & 1) + 0x7FFF
+    return ((u + rounding) >> 16).astype(np.uint16)
+
+
+def bf16_bits_to_float32(b: np.ndarray) -> np.ndarray:
+    return (np.asarray(b, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+class CudaKernel:
+    """Kirchhoff PSTM on one CUDA device (sm_100a) through ``libpstm_cuda.so``.
+
+    Parameters
+    ----------
+    device:
+        CUDA device index (default: ``PSTM_CUDA_DEVICE`` or 0).
+    trace_dtype:
+        ``"auto"`` keeps float32/float16 amplitudes as given and treats uint16
+        arrays as BF16 bit patterns; ``"bf16"``/``"f16"``/``"f32"`` convert on
+        the host first (the precision form stores traces in 16 bits).
+    compensated:
+        Compensated (TwoSum) FP32 accumulation across trace chunks.
+    velocity_mode:
+        ``"exact"`` uses a 3-D velocity slice per pillar; ``"auto"`` follows the
+        Metal host rule (``metal_compiled.py:631-664``): the centre pillar is
+        used for every pillar unless the lateral variation exceeds 5 %.
+    """
+
+    def __init__(self, device: int | None = None, trace_dtype: str = "auto",
+                 compensated: bool = True, velocity_mode: str = "exact"):
+        self._device = int(os.environ.get("PSTM_CUDA_DEVICE", "0")) if device is None else int(device)
+        self._trace_dtype = trace_dtype
+        self._compensated = bool(compensated)
+        self._velocity_mode = velocity_mode
+        self._config = None
+        self._ctx = None
+        self._lib = None
+
+    # ------------------------------------------------------------- protocol
+    @property
+    def name(self) -> str:
+        return "cuda_b200"
+
+    @property
+    def capabilities(self) -> set:
+        try:  # report the reference's own enum members when it is importable
+            from pstm.kernels.base import KernelCapability as RefCap  # type: ignore
+            return {RefCap.FP16, RefCap.ASYNC, RefCap.BATCH}
+        except Exception:
+            return {KernelCapability.FP16, KernelCapability.ASYNC, KernelCapability.BATCH}
+
+    def initialize(self, config) -> None:
+        self._lib = nat.load()
+        if self._ctx is None:
+            h = ctypes.c_void_p()
+            rc = self._lib.pstm_cuda_create(self._device, ctypes.byref(h))
+            nat.check(rc, None, self._lib)
+            self._ctx = h
+        self._config = config
+
+    def migrate_tile(self, traces, output, velocity, config=None) -> KernelMetrics:
+        return self._migrate(traces, output, velocity, config, nat.TT_STRAIGHT)
+
+    def migrate_tile_curved_ray(self, traces, output, velocity, config=None) -> KernelMetrics:
+        return self._migrate(traces, output, velocity, config, nat.TT_CURVED)
+
+    def migrate_tile_vti(self, traces, output, velocity, config=None) -> KernelMetrics:
+        return self._migrate(traces, output, velocity, config, nat.TT_VTI)
+
+    def migrate_tile_curved_vti(self, traces, output, velocity, config=None) -> KernelMetrics:
+        return self._migrate(traces, output, velocity, config, nat.TT_CURVED_VTI)
+
+    def synchronize(self) -> None:
+        if self._ctx is not None:
+            nat.check(self._lib.pstm_cuda_synchronize(self._ctx), self._ctx, self._lib)
+
+    def cleanup(self) -> None:
+        if self._ctx is not None:
+            self._lib.pstm_cuda_destroy(self._ctx)
+        self._ctx = None
+        self._config = None
+
+    def __del__(self):
+        try:
+            self.cleanup()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------- internals
+    @property
+    def context(self):
+        return self._ctx
+
+    def _params(self, cfg, tt: int, keep: list, eta_override=None) -> nat.Params:
+        p = nat.Params()
+        p.max_aperture_m = float(cfg.max_aperture_m)
+        p.min_aperture_m = float(cfg.min_aperture_m)
+        p.max_dip_degrees = float(cfg.max_dip_degrees)
+        p.taper_fraction = float(cfg.taper_fraction)
+        p.apply_spreading = int(bool(cfg.apply_spreading))
+        p.apply_obliquity = int(bool(cfg.apply_obliquity))
+        p.aa_enabled = int(bool(cfg.aa_enabled))
+        p.traveltime = int(tt)
+        p.aa_dominant_freq = float(getattr(cfg, "aa_dominant_freq", 30.0))
+        p.grid_dx = float(getattr(cfg, "grid_dx", 25.0))
+        p.grid_dy = float(getattr(cfg, "grid_dy", 12.5))
+        p.curved_v0 = float(getattr(cfg, "curved_ray_v0", 1500.0))
+        p.curved_k = float(getattr(cfg, "curved_ray_k", 0.5))
+        p.eta_constant = float(getattr(cfg, "vti_eta_constant", 0.0))
+        p.compensated = int(self._compensated)
+        eta = eta_override if eta_override is not None else getattr(cfg, "vti_eta_array", None)
+        if eta is not None and tt in (nat.TT_VTI, nat.TT_CURVED_VTI):
+            ptr, _ = self._arr(eta, np.float64, keep)
+            p.eta = ptr
+            p.eta_is_3d = 0 if len(eta.shape) == 1 else 1
+        return p
+
+    def _arr(self, a, dtype, keep: list):
+        """(pointer, on_device) for a numpy array or a CUDA torch tensor."""
+        if a is None:
+            return None, False
+        if _is_torch_cuda(a):
+            if not a.is_contiguous():
+                a = a.contiguous()
+                keep.append(a)
+            return a.data_ptr(), True
+        arr = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(arr)
+        return arr.ctypes.data, False
+
+    def _amplitudes(self, amps, keep: list):
+        if _is_torch_cuda(amps):
+            import torch
+            code = {torch.float32: nat.AMP_F32, torch.float16: nat.AMP_F16,
+                    torch.bfloat16: nat.AMP_BF16}.get(amps.dtype)
+            if code is None:
+                raise ValueError(f"unsupported amplitude dtype {amps.dtype}")
+            if amps.dim() != 2 or amps.stride(1) != 1:
+                raise ValueError("amplitudes must be (n_traces, n_samples) with unit sample stride")
+            return amps.data_ptr(), code, int(amps.stride(0)), True
+        a = np.asarray(amps)
+        want = self._trace_dtype
+        if want == "bf16" and a.dtype != np.uint16:
+            a = float32_to_bf16_bits(a)
+        elif want == "f16" and a.dtype != np.float16:
+            a = a.astype(np.float16)
+        elif want == "f32" and a.dtype != np.float32:
+            a = a.astype(np.float32)
+        if a.dtype == np.float32:
+            code = nat.AMP_F32
+        elif a.dtype == np.float16:
+            code = nat.AMP_F16
+        elif a.dtype == np.uint16:
+            code = nat.AMP_BF16
+        else:
+            a = a.astype(np.float32)
+            code = nat.AMP_F32
+        if a.ndim != 2 or a.strides[1] != a.itemsize:
+            a = np.ascontiguousarray(a)
+        keep.append(a)
+        return a.ctypes.data, code, a.strides[0] // a.itemsize, False
+
+    def _velocity(self, velocity, output, nx, ny, nt, keep: list):
+        v = velocity.vrms
+        is_1d = bool(getattr(velocity, "is_1d", True))
+        if _is_torch_cuda(v):
+            if (is_1d and tuple(v.shape) != (nt,)) or (not is_1d and tuple(v.shape) != (nx, ny, nt)):
+                raise ValueError("device velocity must match the output tile shape")
+            return self._arr(v, np.float64, keep)[0], (0 if is_1d else 1), True
+        v = np.asarray(v, dtype=np.float64)
+        t_out = np.asarray(output.t_axis_ms, dtype=np.float64)
+        if is_1d:
+            if len(v) != nt:   # numba_cpu_optimized.py:574-578
+                vt = getattr(velocity, "t_axis_ms", None)
+                vt = t_out if vt is None else np.asarray(vt, dtype=np.float64)
+                v = np.interp(t_out, vt, v)
+            is3d = 0
+        else:
+            if v.shape != (nx, ny, nt):
+                raise ValueError(f"3-D velocity shape {v.shape} != tile {(nx, ny, nt)}")
+            is3d = 1
+            if self._velocity_mode == "auto":
+                centre = v[nx // 2, ny // 2, :]
+                rel = np.abs(v - centre[None, None, :]).max() / centre.mean()
+                if rel <= 0.05:
+                    v, is3d = centre, 0
+        if not np.all(v > 0):
+            raise ValueError("velocity must be > 0")
+        v = np.ascontiguousarray(v)
+        keep.append(v)
+        return v.ctypes.data, is3d, False
+
+    def _migrate(self, traces, output, velocity, config, tt: int) -> KernelMetrics:
+        if self._ctx is None or self._config is None:
+            raise RuntimeError("Kernel not initialized")
+        cfg = config if config is not None else self._config
+        t_start = time.perf_counter()
+        keep: list = []
+        nx, ny, nt = len(output.x_axis), len(output.y_axis), len(output.t_axis_ms)
+        ntr = int(traces.amplitudes.shape[0])
+        ns = int(traces.amplitudes.shape[1])
+
+        amp_ptr, amp_code, amp_stride, amp_dev = self._amplitudes(traces.amplitudes, keep)
+        td = nat.TracesDesc()
+        td.amplitudes = amp_ptr
+        td.amp_dtype = amp_code
+        td.n_samples = ns
+        td.n_traces = ntr
+        td.amp_row_stride = amp_stride
+        devs = [amp_dev]
+        for name in ("source_x", "source_y", "receiver_x", "receiver_y", "midpoint_x", "midpoint_y"):
+            ptr, d = self._arr(getattr(traces, name), np.float64, keep)
+            setattr(td, name, ptr)
+            devs.append(d)
+        w = getattr(traces, "weights", None)
+        if w is not None:
+            ptr, d = self._arr(w, np.float64, keep)
+            td.weights = ptr
+            devs.append(d)
+        td.sample_rate_ms = float(traces.sample_rate_ms)
+        td.start_time_ms = float(traces.start_time_ms)
+
+        od = nat.OutputDesc()
+        img = output.image
+        if _is_torch_cuda(img):
+            import torch
+            if img.dtype not in (torch.float64, torch.float32) or not img.is_contiguous():
+                raise ValueError("device image must be a contiguous float64/float32 tensor")
+            od.image = img.data_ptr()
+            od.image_dtype = nat.IMAGE_F64 if img.dtype == torch.float64 else nat.IMAGE_F32
+            devs.append(True)
+        else:
+            if not isinstance(img, np.ndarray) or img.dtype not in (np.float64, np.float32) \
+                    or not img.flags["C_CONTIGUOUS"]:
+                raise ValueError("image must be a C-contiguous float64/float32 array")
+            od.image = img.ctypes.data
+            od.image_dtype = nat.IMAGE_F64 if img.dtype == np.float64 else nat.IMAGE_F32
+            devs.append(False)
+        if tuple(img.shape) != (nx, ny, nt):
+            raise ValueError(f"image shape {tuple(img.shape)} != {(nx, ny, nt)}")
+        fold = output.fold
+        if fold is not None:
+            if _is_torch_cuda(fold):
+                od.fold = fold.data_ptr()
+                devs.append(True)
+            else:
+                if not isinstance(fold, np.ndarray) or fold.dtype != np.int32 or not fold.flags["C_CONTIGUOUS"]:
+                    raise ValueError("fold must be a C-contiguous int32 array")
+                od.fold = fold.ctypes.data
+                devs.append(False)
+            od.fold_is_3d = 1 if len(fold.shape) == 3 else 0
+        od.nx, od.ny, od.nt = nx, ny, nt
+        od.x_axis, d1 = self._arr(output.x_axis, np.float64, keep)
+        od.y_axis, d2 = self._arr(output.y_axis, np.float64, keep)
+        od.t_axis_ms, d3 = self._arr(output.t_axis_ms, np.float64, keep)
+        devs += [d1, d2, d3]
+        xg, yg = getattr(output, "x_grid", None), getattr(output, "y_grid", None)
+        if xg is not None and yg is not None:
+            od.x_grid, d4 = self._arr(xg, np.float64, keep)
+            od.y_grid, d5 = self._arr(yg, np.float64, keep)
+            devs += [d4, d5]
+
+        vd = nat.VelocityDesc()
+        vd.vrms, vd.is_3d, dv = self._velocity(velocity, output, nx, ny, nt, keep)
+        devs.append(dv)
+        prm = self._params(cfg, tt, keep)
+
+        on_dev = all(devs)
+        if any(devs) and not on_dev:
+            raise ValueError("mixing device tensors and host arrays in one call is not supported")
+        if on_dev:
+            import torch   # order the launch after the producers of the caller's tensors
+            stream = torch.cuda.current_stream().cuda_stream
+            rc = self._lib.pstm_cuda_migrate_tile_dev(self._ctx, ctypes.byref(td), ctypes.byref(od),
+                                                      ctypes.byref(vd), ctypes.byref(prm),
+                                                      ctypes.c_void_p(stream))
+        else:
+            rc = self._lib.pstm_cuda_migrate_tile_host(self._ctx, ctypes.byref(td), ctypes.byref(od),
+                                                       ctypes.byref(vd), ctypes.byref(prm))
+        nat.check(rc, self._ctx, self._lib)
+        return KernelMetrics(n_traces_processed=ntr, n_samples_output=nx * ny * nt,
+                             compute_time_s=time.perf_counter() - t_start)
+
+
+def create_cuda_kernel(**kw) -> CudaKernel:
+    """Factory in the style of ``create_optimized_numba_kernel``."""
+    return CudaKernel(**kw)

@@ -1,0 +1,225 @@
+"""CUDA backend vs the reference's outputs and the FP64 oracle (GPU).
+
+Tolerances (written here, checked below):
+* plain straight-ray, FP32 traces, vs the reference Numba path: fold
+  bit-exact, image relative L2 <= 1e-5;
+* curved / VTI / curved+VTI / AA / 3-D velocity, FP32 traces, vs the FP64
+  oracle: fold bit-exact, image relative L2 <= 1e-4;
+* BF16 / FP16 traces: <= 1e-5 against the oracle fed the same rounded traces,
+  <= 1e-3 against the oracle fed the FP32 traces.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_files, interp_velocity, load_golden_case, rel_l2
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_TOL = 1e-5
+EXACT_KIND_TOL = 1e-4
+BF16_TOL = 1e-3
+
+
+def fresh(out, image_dtype=np.float64, fold_shape=None):
+    from pstm_b200.base import OutputTile
+    nx, ny, nt = len(out.x_axis), len(out.y_axis), len(out.t_axis_ms)
+    return OutputTile(image=np.zeros((nx, ny, nt), image_dtype),
+                      fold=np.zeros(fold_shape or (nx, ny, nt), np.int32),
+                      x_axis=out.x_axis, y_axis=out.y_axis, t_axis_ms=out.t_axis_ms,
+                      x_grid=getattr(out, "x_grid", None), y_grid=getattr(out, "y_grid", None))
+
+
+def oracle_run(case_traces, out, vel, cfg, kind="straight_ray", pillars=None):
+    ref = fresh(out, fold_shape=out.fold.shape)
+    oracle.migrate(case_traces, ref, vel, cfg, kind=kind, pillars=pillars)
+    return ref
+
+
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p)[6:-4])
+def test_matches_reference_numba_golden(path, cuda_kernel_factory):
+    tb, out, vel, cfg, img_ref, fold_ref = load_golden_case(path)
+    k = cuda_kernel_factory(cfg)
+    k.migrate_tile(tb, out, vel)
+    np.testing.assert_array_equal(out.fold, fold_ref)
+    if np.abs(img_ref).max() == 0:
+        assert np.abs(out.image).max() == 0
+    else:
+        assert rel_l2(out.image, img_ref) <= PLAIN_TOL
+
+
+def test_config1_full_tile(cuda_kernel_factory):
+    """Full 64x64x500 tile x 16,384 traces; fold everywhere against an FP64
+    count, image against the oracle on pillars around the three diffractors."""
+    from pstm_b200 import workloads
+    case = workloads.config1()
+    k = cuda_kernel_factory(case.config)
+    k.migrate_tile(case.traces, case.output, case.velocity)
+    tb, out = case.traces, case.output
+    X, Y = np.meshgrid(out.x_axis, out.y_axis, indexing="ij")
+    cnt = np.zeros(X.shape, np.int64)
+    for i in range(0, tb.n_traces, 2048):
+        d = np.sqrt((X[..., None] - tb.midpoint_x[None, None, i:i + 2048]) ** 2 +
+                    (Y[..., None] - tb.midpoint_y[None, None, i:i + 2048]) ** 2)
+        cnt += (~(d > case.config.max_aperture_m)).sum(-1)
+    np.testing.assert_array_equal(out.fold, np.broadcast_to(cnt[..., None], out.fold.shape))
+    ny = out.ny
+    for ix in (32, 20, 48):   # rows through (800,800), (500,1100), (1200,400)
+        ref = oracle_run(tb, out, case.velocity, case.config, pillars=(ix * ny, (ix + 1) * ny))
+        assert rel_l2(out.image[ix], ref.image[ix]) <= PLAIN_TOL
+
+
+def test_device_tensors_match_host_arrays(cuda_kernel_factory):
+    import torch
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    case = workloads.config1(n_traces=2048, nx=24, ny=20, nt=500)
+    k = cuda_kernel_factory(case.config)
+    k.migrate_tile(case.traces, case.output, case.velocity)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()
+    tb = case.traces
+    dtb = TraceBlock(amplitudes=dev(tb.amplitudes), source_x=dev(tb.source_x), source_y=dev(tb.source_y),
+                     receiver_x=dev(tb.receiver_x), receiver_y=dev(tb.receiver_y), offset=dev(tb.offset),
+                     midpoint_x=dev(tb.midpoint_x), midpoint_y=dev(tb.midpoint_y),
+                     sample_rate_ms=tb.sample_rate_ms, start_time_ms=tb.start_time_ms)
+    o = case.output
+    dout = OutputTile(image=torch.zeros(o.image.shape, dtype=torch.float64, device="cuda"),
+                      fold=torch.zeros(o.fold.shape, dtype=torch.int32, device="cuda"),
+                      x_axis=dev(o.x_axis), y_axis=dev(o.y_axis), t_axis_ms=dev(o.t_axis_ms))
+    k.migrate_tile(dtb, dout, VelocitySlice(vrms=dev(case.velocity.vrms), is_1d=True))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dout.fold.cpu().numpy(), o.fold)
+    np.testing.assert_array_equal(dout.image.cpu().numpy(), o.image)
+
+
+@pytest.mark.parametrize("kind", ["straight_ray", "curved_ray", "anisotropic_vti", "curved_vti"])
+@pytest.mark.parametrize("aa", [False, True])
+def test_traveltime_kinds_vs_oracle(kind, aa, cuda_kernel_factory):
+    from pstm_b200 import workloads
+    case = workloads.config2_small()
+    cfg = workloads.survey_config(kernel_type=kind, aa=aa, eta=workloads.survey_eta(case.output.t_axis_ms),
+                                  v0=1500.0, k=0.9)
+    k = cuda_kernel_factory(cfg)
+    method = {"straight_ray": k.migrate_tile, "curved_ray": k.migrate_tile_curved_ray,
+              "anisotropic_vti": k.migrate_tile_vti, "curved_vti": k.migrate_tile_curved_vti}[kind]
+    method(case.traces, case.output, case.velocity)
+    ref = oracle_run(case.traces, case.output, case.velocity, cfg, kind=kind)
+    np.testing.assert_array_equal(case.output.fold, ref.fold)
+    err = rel_l2(case.output.image, ref.image)
+    assert err <= EXACT_KIND_TOL, err
+
+
+def test_curved_zero_gradient_and_constant_eta(cuda_kernel_factory):
+    from pstm_b200 import workloads
+    case = workloads.config2_small(n_traces=1024, nx=8, ny=8)
+    cfg = workloads.survey_config(kernel_type="curved_ray", aa=False, v0=1700.0, k=0.0)
+    k = cuda_kernel_factory(cfg)
+    k.migrate_tile_curved_ray(case.traces, case.output, case.velocity)
+    ref = oracle_run(case.traces, case.output, case.velocity, cfg, kind="curved_ray")
+    assert rel_l2(case.output.image, ref.image) <= EXACT_KIND_TOL
+    cfg2 = workloads.survey_config(kernel_type="anisotropic_vti", aa=False)
+    cfg2.vti_eta_array = None
+    cfg2.vti_eta_constant = 0.12
+    out = fresh(case.output)
+    k.migrate_tile_vti(case.traces, out, case.velocity, cfg2)
+    ref = oracle_run(case.traces, out, case.velocity, cfg2, kind="anisotropic_vti")
+    assert rel_l2(out.image, ref.image) <= EXACT_KIND_TOL
+
+
+@pytest.mark.parametrize("dtype", ["bf16", "f16"])
+def test_16bit_traces(dtype, cuda_kernel_factory):
+    from pstm_b200 import workloads
+    from pstm_b200.cuda_kernel import bf16_bits_to_float32, float32_to_bf16_bits
+    case = workloads.config2_small()
+    k = cuda_kernel_factory(case.config, trace_dtype=dtype)
+    k.migrate_tile(case.traces, case.output, case.velocity)
+    tb = case.traces
+    q = bf16_bits_to_float32(float32_to_bf16_bits(tb.amplitudes)) if dtype == "bf16" \
+        else tb.amplitudes.astype(np.float16).astype(np.float32)
+    import dataclasses
+    tq = dataclasses.replace(tb, amplitudes=q)
+    ref_q = oracle_run(tq, case.output, case.velocity, case.config)
+    ref = oracle_run(tb, case.output, case.velocity, case.config)
+    np.testing.assert_array_equal(case.output.fold, ref.fold)
+    assert rel_l2(case.output.image, ref_q.image) <= PLAIN_TOL
+    assert rel_l2(case.output.image, ref.image) <= BF16_TOL
+
+
+def test_edge_shapes_rotated_grid_f32_image_2d_fold(cuda_kernel_factory):
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile
+    case = workloads.config1(n_traces=700, nx=7, ny=13, nt=37)
+    c = case.config
+    out = case.output
+    X, Y = np.meshgrid(out.x_axis + 300.0, out.y_axis + 200.0, indexing="ij")
+    ang = 0.3
+    Xr = 700 + (X - 700) * np.cos(ang) - (Y - 700) * np.sin(ang)
+    Yr = 700 + (X - 700) * np.sin(ang) + (Y - 700) * np.cos(ang)
+    rot = OutputTile(image=np.zeros(out.image.shape, np.float32), fold=np.zeros(out.image.shape[:2], np.int32),
+                     x_axis=out.x_axis, y_axis=out.y_axis, t_axis_ms=out.t_axis_ms, x_grid=Xr, y_grid=Yr)
+    k = cuda_kernel_factory(c)
+    k.migrate_tile(case.traces, rot, case.velocity)
+    ref = oracle_run(case.traces, rot, case.velocity, c)
+    np.testing.assert_array_equal(rot.fold, ref.fold)
+    assert rel_l2(rot.image, ref.image) <= PLAIN_TOL
+
+
+def test_zero_and_single_trace(cuda_kernel_factory):
+    from pstm_b200 import workloads
+    from pstm_b200.base import create_trace_block
+    case = workloads.config1(n_traces=1, nx=5, ny=5, nt=40)
+    k = cuda_kernel_factory(case.config)
+    k.migrate_tile(case.traces, case.output, case.velocity)
+    ref = oracle_run(case.traces, case.output, case.velocity, case.config)
+    np.testing.assert_array_equal(case.output.fold, ref.fold)
+    assert rel_l2(case.output.image, ref.image) <= PLAIN_TOL
+    empty = create_trace_block(np.zeros((0, 500), np.float32), *([np.zeros(0)] * 4), sample_rate_ms=4.0)
+    before_i, before_f = case.output.image.copy(), case.output.fold.copy()
+    k.migrate_tile(empty, case.output, case.velocity)
+    np.testing.assert_array_equal(case.output.image, before_i)
+    np.testing.assert_array_equal(case.output.fold, before_f)
+
+
+def test_additive_over_trace_splits_and_exact_scaling(cuda_kernel_factory):
+    """Size-independent properties: fold and image add over a split of the
+    traces; scaling the traces by 2 scales the image by exactly 2."""
+    import dataclasses
+    from pstm_b200 import workloads
+    case = workloads.config1(n_traces=6000, nx=16, ny=16, nt=500)
+    k = cuda_kernel_factory(case.config)
+    tb = case.traces
+    k.migrate_tile(tb, case.output, case.velocity)
+    split = fresh(case.output)
+    half = tb.n_traces // 2
+    for sl in (slice(0, half), slice(half, None)):
+        part = dataclasses.replace(tb, **{f: getattr(tb, f)[sl] for f in
+                                          ("amplitudes", "source_x", "source_y", "receiver_x", "receiver_y",
+                                           "offset", "midpoint_x", "midpoint_y")})
+        k.migrate_tile(part, split, case.velocity)
+    np.testing.assert_array_equal(split.fold, case.output.fold)
+    assert rel_l2(split.image, case.output.image) <= 1e-6
+    doubled = fresh(case.output)
+    k.migrate_tile(dataclasses.replace(tb, amplitudes=tb.amplitudes * 2), doubled, case.velocity)
+    np.testing.assert_allclose(doubled.image, 2 * case.output.image, rtol=1e-6, atol=0)
+
+
+def test_invalid_arguments_and_injected_fault(cuda_kernel_factory, monkeypatch):
+    from pstm_b200 import workloads
+    from pstm_b200._native import PstmCudaError
+    case = workloads.config1(n_traces=64, nx=4, ny=4, nt=20)
+    k = cuda_kernel_factory(case.config)
+    bad = workloads.config1(n_traces=64, nx=4, ny=4, nt=20)
+    bad.velocity.vrms[:] = 0.0
+    with pytest.raises(ValueError):
+        k.migrate_tile(bad.traces, bad.output, bad.velocity)
+    monkeypatch.setenv("PSTM_CUDA_INJECT_FAULT", "migrate")
+    with pytest.raises(PstmCudaError, match="INJECTED"):
+        k.migrate_tile(case.traces, case.output, case.velocity)
+    monkeypatch.delenv("PSTM_CUDA_INJECT_FAULT")
+    k.migrate_tile(case.traces, case.output, case.velocity)   # context still usable
+    ref = oracle_run(case.traces, case.output, case.velocity, case.config)
+    assert rel_l2(case.output.image, ref.image) <= PLAIN_TOL
