@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--dtype", choices=["f32", "bf16", "f16"], default="f32")
+    ap.add_argument("--precision", choices=["exact", "fast"], default="exact")
     ap.add_argument("--traces", type=int, default=1 << 20)
     ap.add_argument("--tile", type=int, default=64)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -224,7 +225,7 @@ def main_ours(args):
         tile_args[tl] = (OutputTile(image=img, fold=fold, x_axis=dev(sv.x_axis[ix0:ix1]),
                                     y_axis=dev(sv.y_axis[iy0:iy1]), t_axis_ms=t_axis),
                          VelocitySlice(vrms=dev(sv.velocity(ix0, ix1, iy0, iy1)), is_1d=False))
-    k = CudaKernel()
+    k = CudaKernel(precision=args.precision)
     k.initialize(cfg)
     pairs_per_step = T * T * NT * N
 
@@ -303,7 +304,7 @@ def main_ours(args):
             h_tiles[tl] = (OutputTile(image=h_img, fold=h_fold, x_axis=sv.x_axis[ix0:ix1], y_axis=sv.y_axis[iy0:iy1],
                                       t_axis_ms=sv.t_axis_ms),
                            VelocitySlice(vrms=pinned(sv.velocity(ix0, ix1, iy0, iy1)), is_1d=False))
-        ke = CudaKernel(trace_dtype="auto")
+        ke = CudaKernel(trace_dtype="auto", precision=args.precision)
         ke.initialize(cfg)
         ke.migrate_tile(htb, *h_tiles[my_tiles[0]])   # warm the staging buffers
         if dist:
@@ -345,7 +346,7 @@ def main_ours(args):
                                    "3.2 km patch, 3-D v_rms, AA on, 5 km aperture; one step = "
                                    f"{T}x{T}x{NT} output tile (pillars x samples)",
                        "traces": N, "tile": [T, T, NT], "grid": [GRID, GRID, NT], "traveltime": "straight_ray",
-                       "trace_dtype": args.dtype, "accumulate": "fp32 compensated -> f64 image",
+                       "trace_dtype": args.dtype, "precision": args.precision, "accumulate": "fp32 compensated -> f64 image",
                        "l2": "inputs larger than L2 (trace panel > 126 MB), no flush",
                        "parallelism": f"replicas x{world} (disjoint tiles)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

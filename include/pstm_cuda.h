@@ -42,6 +42,12 @@ typedef enum {
 } pstm_status;
 
 typedef enum { PSTM_AMP_F32 = 0, PSTM_AMP_BF16 = 1, PSTM_AMP_F16 = 2 } pstm_amp_dtype;
+
+/* Traveltime arithmetic of the straight-ray kernel.  EXACT forms the
+ * fractional sample index in FP64 (the reference Numba path's precision for
+ * the interpolation position and the trace-end test); FAST uses FP32
+ * traveltime (the precision form).  Weights and accumulation are FP32 in both. */
+typedef enum { PSTM_PREC_EXACT = 0, PSTM_PREC_FAST = 1 } pstm_precision;
 typedef enum { PSTM_IMAGE_F64 = 0, PSTM_IMAGE_F32 = 1 } pstm_image_dtype;
 
 /* Traveltime kinds.  Reference: executor dispatch pstm/pipeline/executor.py:1691-1745
@@ -50,7 +56,7 @@ typedef enum {
     PSTM_TT_STRAIGHT = 0,    /* DSR, numba_cpu_optimized.py:192-194 */
     PSTM_TT_CURVED = 1,      /* V(z)=v0+kz, pstm_curved_ray.metal:50-96 */
     PSTM_TT_VTI = 2,         /* eta moveout, pstm_anisotropic_vti.metal:103-148 */
-    PSTM_TT_CURVED_VTI = 3   /* curved leg with the VTI quartic correction (no reference formula) */
+    PSTM_TT_CURVED_VTI = 3   /* curved leg x VTI/hyperbolic leg ratio (no reference formula) */
 } pstm_traveltime;
 
 /* Trace panel + geometry.  Reference carrier: TraceBlock, pstm/kernels/base.py:27-116. */
@@ -106,6 +112,8 @@ typedef struct {
     int32_t eta_is_3d;
     int32_t compensated;          /* 1: compensated (TwoSum) FP32 accumulation */
     double eta_constant;
+    int32_t precision;            /* pstm_precision; straight rays only, others are FP32 */
+    int32_t reserved;
 } pstm_params;
 
 /* Library / ABI version (no reference counterpart: a binding sanity check). */
@@ -121,7 +129,9 @@ int32_t pstm_cuda_create(int32_t device, void **ctx_out);
 void pstm_cuda_destroy(void *ctx);
 
 /* Migrate one tile, device pointers, asynchronous on `stream` (a
- * cudaStream_t; NULL = the context's stream).  Replaces
+ * cudaStream_t; NULL = the context's stream; pass cudaStreamLegacy, 0x1, for
+ * the legacy default stream).  Calls on one context must not overlap on the
+ * device: the context's per-launch tables are reused by the next call.  Replaces
  * MigrationKernel.migrate_tile, base.py:305-313;
  * OptimizedNumbaKernel.migrate_tile, numba_cpu_optimized.py:545-626;
  * CompiledMetalKernel.migrate_tile[_curved_ray/_vti], metal_compiled.py:567,1275,1456. */

@@ -23,8 +23,10 @@
  *       pstm/algorithm/anisotropy_vti.py:148-220
  *       pstm/metal/shaders/pstm_anisotropic_vti.metal:103-148, :252-333
  *   curved-ray + VTI: the reference has no combined formula; this build
- *       defines it as the VTI quartic correction (with the NMO velocity
- *       v_rms(t)) subtracted from the squared curved-ray leg time.
+ *       defines each leg as the curved-ray leg time scaled by the VTI /
+ *       hyperbolic ratio of the same leg in the NMO velocity v_rms(t):
+ *       t = t_curved * sqrt(1 - corr / (t0h^2 + h^2/v^2)), which is t_curved
+ *       at eta = 0 and never cancels (corr < h^2/v^2).
  *
  * Fold follows the Numba path for every traveltime kind: per pillar, the
  * number of traces whose midpoint lies within max_aperture, added to every
@@ -134,8 +136,9 @@ static double leg_curved_vti(double t0h, double h, double z, double v0, double k
 {
     double tc = leg_curved(h, z, v0, k);
     if (v <= 0.0 || t0h <= 0.0) return tc;
-    double t2 = tc * tc - vti_correction(t0h, h, v, eta);
-    return sqrt(t2 > 0.0 ? t2 : 0.0);
+    double hyp = t0h * t0h + (h * h) / (v * v);
+    double r = 1.0 - vti_correction(t0h, h, v, eta) / hyp;
+    return tc * sqrt(r > 0.0 ? r : 0.0);
 }
 
 /* compute_aa_weight, pstm_migration.metal:95-132 */

@@ -26,6 +26,8 @@ STATUS_NAMES = {
 AMP_F32, AMP_BF16, AMP_F16 = 0, 1, 2
 IMAGE_F64, IMAGE_F32 = 0, 1
 TT_STRAIGHT, TT_CURVED, TT_VTI, TT_CURVED_VTI = 0, 1, 2, 3
+PREC_EXACT, PREC_FAST = 0, 1
+STREAM_LEGACY = 1   # cudaStreamLegacy
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -62,7 +64,7 @@ class Params(ctypes.Structure):
         ("aa_dominant_freq", ctypes.c_double), ("grid_dx", ctypes.c_double),
         ("grid_dy", ctypes.c_double), ("curved_v0", ctypes.c_double), ("curved_k", ctypes.c_double),
         ("eta", _vp), ("eta_is_3d", ctypes.c_int32), ("compensated", ctypes.c_int32),
-        ("eta_constant", ctypes.c_double),
+        ("eta_constant", ctypes.c_double), ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 

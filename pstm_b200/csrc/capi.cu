@@ -14,8 +14,8 @@
 
 namespace pstm {
 template <int TT>
-cudaError_t launch_migrate_tt(const KParams &, int, bool, bool, const TileShape &, dim3, cudaStream_t);
-__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab);
+cudaError_t launch_migrate_tt(const KParams &, const KParams *, int, bool, bool, bool, const TileShape &, dim3,
+                              size_t, cudaStream_t);
 }  // namespace pstm
 
 using namespace pstm;
@@ -31,17 +31,14 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    DevBuf ttab;
+    DevBuf ttab, btab, kparams, errword;
     // staging for the host-pointer path
     DevBuf amps, geo[7], xa, ya, xg, yg, ta, vel, eta, image, fold;
-    TileShape shape{2, 8, 64};
+    TileShape shape{2, 4};
+    int smem_optin = 0;   // max dynamic shared memory per block
 };
 
 thread_local std::string g_create_err;
-
-struct Status {
-    int32_t code;
-};
 
 int32_t fail(Ctx *c, int32_t code, const std::string &msg) {
     if (c) c->err = msg;
@@ -116,6 +113,8 @@ int32_t validate(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out
     if (!vel->vrms) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null velocity");
     if (prm->traveltime < PSTM_TT_STRAIGHT || prm->traveltime > PSTM_TT_CURVED_VTI)
         return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown traveltime kind");
+    if (prm->precision != PSTM_PREC_EXACT && prm->precision != PSTM_PREC_FAST)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown precision");
     if (!(prm->max_aperture_m >= 0.0) || !(prm->taper_fraction >= 0.0) || !(prm->taper_fraction <= 1.0))
         return fail(c, PSTM_ERR_INVALID_ARGUMENT, "bad aperture/taper parameters");
     if ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) && !(prm->curved_v0 > 0.0))
@@ -131,6 +130,7 @@ KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, con
     P.amp_stride = tr->amp_row_stride;
     P.n_traces = tr->n_traces;
     P.ns = tr->n_samples;
+    P.elem = (int32_t)amp_elem_bytes(tr->amp_dtype);
     P.sx = tr->source_x; P.sy = tr->source_y;
     P.rx = tr->receiver_x; P.ry = tr->receiver_y;
     P.mx = tr->midpoint_x; P.my = tr->midpoint_y;
@@ -146,6 +146,7 @@ KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, con
     P.s_rej_lo = -g;
     P.s_rej_hi = smax + g;
     P.s_max_clamp = std::nextafter(smax, 0.0f);
+    P.s_magic = 2147483648.0 - P.tstart_s / P.dt_s;
 
     P.image = out->image;
     P.fold = out->fold;
@@ -184,9 +185,10 @@ KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, con
     P.compensated = prm->compensated ? 1 : 0;
 
     // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)
-    int py = sh.PB, px = 1;
+    const int PB = sh.PBG * kWarpsP;
+    int py = PB, px = 1;
     while (py > 1 && py > out->ny) { py /= 2; px *= 2; }
-    if (py == sh.PB && sh.PB >= 4) { py = sh.PB / 2; px = 2; }
+    if (py == PB && PB >= 4) { py = PB / 2; px = 2; }
     P.px = px;
     P.py = py;
     P.n_pblk_y = (out->ny + py - 1) / py;
@@ -205,32 +207,81 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
 
     const bool per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
     const int64_t n_p = per_pillar ? (int64_t)out->nx * out->ny : 1;
-    e = ensure(c->ttab, (size_t)n_p * out->nt * sizeof(float4));
-    if (e != cudaSuccess) return cuda_fail(c, e, "allocating the time table");
+    const size_t n_tab = (size_t)n_p * out->nt;
+    if ((e = ensure(c->ttab, n_tab * sizeof(float4))) != cudaSuccess ||
+        (e = ensure(c->btab, n_tab * sizeof(double))) != cudaSuccess ||
+        (e = ensure(c->errword, sizeof(int32_t))) != cudaSuccess)
+        return cuda_fail(c, e, "allocating the per-time tables");
     float4 *tab = reinterpret_cast<float4 *>(c->ttab.ptr);
+    double *btab = reinterpret_cast<double *>(c->btab.ptr);
     {
-        const int64_t n = n_p * out->nt;
-        int blocks = (int)((n + 255) / 256);
+        int blocks = (int)(((int64_t)n_tab + 255) / 256);
         if (blocks > 148 * 32) blocks = 148 * 32;
-        prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab);
+        prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab, btab);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(c, e, "prep_time_table launch");
     }
     P.ttab = tab;
+    P.btab = btab;
+    P.err = reinterpret_cast<int32_t *>(c->errword.ptr);
+    if ((e = cudaMemsetAsync(P.err, 0, sizeof(int32_t), st)) != cudaSuccess)
+        return cuda_fail(c, e, "clearing the error word");
 
+    // shared-memory staging of trace rows: pitch rounded up to 16 bytes; TMA
+    // bulk copies when the rows are 16-byte aligned and the padded row is
+    // inside the caller's stride, else a plain cooperative copy
+    const int eb = P.elem;
+    const int per16 = 16 / eb;
+    const int pitch = (tr->n_samples + per16 - 1) / per16 * per16;
+    const bool aligned = ((uintptr_t)tr->amplitudes % 16 == 0) && ((tr->amp_row_stride * eb) % 16 == 0);
+    P.pitch = pitch;
+    P.bulk = (aligned && tr->amp_row_stride >= pitch) ? 1 : 0;
     const TileShape &sh = c->shape;
+    const int PB = sh.PBG * kWarpsP;
+    const bool exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
+    const int nrec = prm->traveltime == PSTM_TT_CURVED_VTI ? 3
+                     : (prm->traveltime == PSTM_TT_STRAIGHT && !prm->aa_enabled) ? 1 : 2;
+    const size_t rec_bytes = (size_t)records_bytes(PB, nrec, exact);
+    const size_t static_bytes = 2048;   // s_ox/s_oy/s_pid/s_fold/barriers, rounded up
+    const size_t budget = (size_t)c->smem_optin > rec_bytes + static_bytes ? c->smem_optin - rec_bytes - static_bytes : 0;
+    int chunk = (int)(budget / (2 * (size_t)pitch * eb));
+    if (chunk > kMaxChunk) chunk = kMaxChunk;
+    if (chunk < 1) return fail(c, PSTM_ERR_UNSUPPORTED, "trace rows too long to stage in shared memory");
+    P.chunk = chunk;
+    const size_t smem = 2 * (size_t)chunk * pitch * eb + rec_bytes;
+
+    // a device copy of the launch parameters for the kernel's rare FP64 paths
+    e = ensure(c->kparams, sizeof(KParams));
+    if (e != cudaSuccess) return cuda_fail(c, e, "allocating the parameter block");
+    e = cudaMemcpyAsync(c->kparams.ptr, &P, sizeof(KParams), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "copying the parameter block");
+    const KParams *Pg = reinterpret_cast<const KParams *>(c->kparams.ptr);
+
     const int n_pblk_x = (out->nx + P.px - 1) / P.px;
     const int64_t nblk_p = (int64_t)n_pblk_x * P.n_pblk_y;
-    const int nblk_t = (out->nt + kThreads * sh.R - 1) / (kThreads * sh.R);
+    const int tb = kWarpsT * 32 * sh.R;
+    const int nblk_t = (out->nt + tb - 1) / tb;
     if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(c, PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
     dim3 grid((unsigned)nblk_p, (unsigned)nblk_t);
+    const bool aa = prm->aa_enabled != 0;
     switch (prm->traveltime) {
-    case PSTM_TT_STRAIGHT: e = launch_migrate_tt<TT_STRAIGHT>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
-    case PSTM_TT_CURVED: e = launch_migrate_tt<TT_CURVED>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
-    case PSTM_TT_VTI: e = launch_migrate_tt<TT_VTI>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
-    default: e = launch_migrate_tt<TT_CURVED_VTI>(P, tr->amp_dtype, per_pillar, prm->aa_enabled != 0, sh, grid, st); break;
+    case PSTM_TT_STRAIGHT: e = launch_migrate_tt<TT_STRAIGHT>(P, Pg, tr->amp_dtype, per_pillar, aa, exact, sh, grid, smem, st); break;
+    case PSTM_TT_CURVED: e = launch_migrate_tt<TT_CURVED>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
+    case PSTM_TT_VTI: e = launch_migrate_tt<TT_VTI>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
+    default: e = launch_migrate_tt<TT_CURVED_VTI>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "migrate kernel launch");
+    return PSTM_OK;
+}
+
+// Read back the kernels' error word (after the stream has drained).
+int32_t check_error_word(Ctx *c) {
+    if (!c->errword.ptr) return PSTM_OK;
+    int32_t w = 0;
+    cudaError_t e = cudaMemcpy(&w, c->errword.ptr, sizeof(w), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(c, e, "reading the error word");
+    if (w & KERR_WAIT_TIMEOUT)
+        return fail(c, PSTM_ERR_TIMEOUT, "a bounded wait for a trace-row copy gave up; the tile was not written");
     return PSTM_OK;
 }
 
@@ -270,10 +321,16 @@ int32_t pstm_cuda_create(int32_t device, void **ctx_out) {
         delete c;
         return cuda_fail(nullptr, e, "cudaStreamCreate");
     }
-    const char *shape = std::getenv("PSTM_CUDA_TILE");   // "R,PB,C" override
+    e = cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return cuda_fail(nullptr, e, "cudaDeviceGetAttribute");
+    }
+    const char *shape = std::getenv("PSTM_CUDA_TILE");   // "R,PBG" override
     if (shape) {
-        int r, pb, cc;
-        if (std::sscanf(shape, "%d,%d,%d", &r, &pb, &cc) == 3) c->shape = TileShape{r, pb, cc};
+        int r, pbg;
+        if (std::sscanf(shape, "%d,%d", &r, &pbg) == 2) c->shape = TileShape{r, pbg};
     }
     *ctx_out = c;
     return PSTM_OK;
@@ -285,6 +342,9 @@ void pstm_cuda_destroy(void *ctx) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     release(c->ttab);
+    release(c->btab);
+    release(c->kparams);
+    release(c->errword);
     release(c->amps);
     for (auto &g : c->geo) release(g);
     release(c->xa); release(c->ya); release(c->xg); release(c->yg); release(c->ta);
@@ -332,14 +392,17 @@ static int32_t migrate_host_impl(Ctx *c, const pstm_traces_desc *traces, const p
     const size_t eb = amp_elem_bytes(traces->amp_dtype);
     // amplitudes: packed to n_samples per row on the device
     if (N > 0) {
-        e = ensure(c->amps, (size_t)N * traces->n_samples * eb);
+        // rows padded to a 16-byte pitch so the kernel can stage them with TMA bulk copies
+        const size_t per16 = 16 / eb;
+        const size_t pitch = ((size_t)traces->n_samples + per16 - 1) / per16 * per16;
+        e = ensure(c->amps, (size_t)N * pitch * eb);
         if (e != cudaSuccess) return cuda_fail(c, e, "staging amplitudes");
-        e = cudaMemcpy2DAsync(c->amps.ptr, traces->n_samples * eb, traces->amplitudes,
+        e = cudaMemcpy2DAsync(c->amps.ptr, pitch * eb, traces->amplitudes,
                               traces->amp_row_stride * eb, traces->n_samples * eb, (size_t)N,
                               cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return cuda_fail(c, e, "copying amplitudes");
         dt.amplitudes = c->amps.ptr;
-        dt.amp_row_stride = traces->n_samples;
+        dt.amp_row_stride = (int64_t)pitch;
     }
     const double *src_geo[7] = {traces->source_x, traces->source_y, traces->receiver_x, traces->receiver_y,
                                 traces->midpoint_x, traces->midpoint_y, traces->weights};
@@ -387,7 +450,7 @@ static int32_t migrate_host_impl(Ctx *c, const pstm_traces_desc *traces, const p
         (e = cudaMemcpyAsync(output->fold, c->fold.ptr, fold_bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(c, e, "reading fold back");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(c, e, "migrate_tile");
-    return PSTM_OK;
+    return check_error_word(c);
 }
 
 int32_t pstm_cuda_synchronize(void *ctx) {
@@ -397,7 +460,7 @@ int32_t pstm_cuda_synchronize(void *ctx) {
     cudaError_t e = cudaSetDevice(c->device);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "synchronize");
-    return PSTM_OK;
+    return check_error_word(c);
 }
 
 const char *pstm_cuda_last_error(void *ctx) {

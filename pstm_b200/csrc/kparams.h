@@ -2,11 +2,15 @@
 // migration kernels.  Plain C++ struct passed by value to every launch.
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>
 
 namespace pstm {
 
 enum AmpKind { AMP_F32 = 0, AMP_BF16 = 1, AMP_F16 = 2 };
 enum TTKind { TT_STRAIGHT = 0, TT_CURVED = 1, TT_VTI = 2, TT_CURVED_VTI = 3 };
+
+// error bits a kernel can raise in *err
+enum KernelError { KERR_WAIT_TIMEOUT = 1 };
 
 struct KParams {
     // ---- traces ----
@@ -14,7 +18,7 @@ struct KParams {
     int64_t amp_stride;          // elements between rows
     int64_t n_traces;
     int32_t ns;                  // samples per trace
-    int32_t pad0;
+    int32_t elem;                // bytes per amplitude
     const double *sx, *sy, *rx, *ry, *mx, *my, *w;   // w nullable
     double dt_s, tstart_s;       // input sampling (seconds)
     float s_scale, s_offset;     // sample index s = T * s_scale + s_offset
@@ -22,6 +26,13 @@ struct KParams {
     float s_rej_lo, s_rej_hi;    // outside [s_rej_lo, s_rej_hi] the pair is rejected
     float s_max_clamp;           // largest s allowed for the interpolation read
     int32_t pad1;
+    double s_magic;              // 2^31 - tstart/dt: FP64 sample index + 2^31 (EXACT path)
+
+    // ---- staging of trace rows in shared memory ----
+    int32_t chunk;               // traces per chunk (<= kMaxChunk)
+    int32_t pitch;               // staged row pitch, elements (multiple of 16 bytes)
+    int32_t bulk;                // 1: rows are copied by TMA bulk copies
+    int32_t pad2;
 
     // ---- output ----
     void *image;
@@ -37,7 +48,8 @@ struct KParams {
     const double *vrms;          // (nt) or (nx*ny*nt), FP64 (exact paths)
     int32_t vel3d;
     int32_t eta3d;
-    const float4 *ttab;          // per (pillar|0, t): {iv2, ap, eta, 1/v}
+    const float4 *ttab;          // per (pillar|0, t): {1/v^2, aperture, 1/v, eta}
+    const double *btab;          // per (pillar|0, t): 1/(v dt)^2 (EXACT path)
     const double *eta;           // nullable (FP64, exact paths)
     double eta_const;
 
@@ -53,7 +65,7 @@ struct KParams {
     float cr_v0f, cr_kf, cr_inv_k_ln2;   // inv_k * ln2 (log2 based)
     int32_t cr_k_zero;           // |k| < 1e-10: straight-ray fallback with v0
     int32_t compensated;
-    int32_t pad2;
+    int32_t *err;                // device error word (KernelError bits)
 };
 
 }  // namespace pstm

@@ -1,5 +1,6 @@
 // Instantiations of the gather kernel for traveltime kind 0.
 #include "migrate_dispatch.cuh"
 namespace pstm {
-template cudaError_t launch_migrate_tt<0>(const KParams &, int, bool, bool, const TileShape &, dim3, cudaStream_t);
+template cudaError_t launch_migrate_tt<0>(const KParams &, const KParams *, int, bool, bool, bool,
+                                            const TileShape &, dim3, size_t, cudaStream_t);
 }

@@ -71,14 +71,21 @@ class CudaKernel:
         ``"exact"`` uses a 3-D velocity slice per pillar; ``"auto"`` follows the
         Metal host rule (``metal_compiled.py:631-664``): the centre pillar is
         used for every pillar unless the lateral variation exceeds 5 %.
+    precision:
+        ``"exact"`` forms the straight-ray sample index in FP64 (the reference
+        Numba path's interpolation position); ``"fast"`` uses FP32 traveltime
+        (the precision form).  Curved-ray and VTI kernels are FP32 either way.
     """
 
     def __init__(self, device: int | None = None, trace_dtype: str = "auto",
-                 compensated: bool = True, velocity_mode: str = "exact"):
+                 compensated: bool = True, velocity_mode: str = "exact", precision: str = "exact"):
         self._device = int(os.environ.get("PSTM_CUDA_DEVICE", "0")) if device is None else int(device)
         self._trace_dtype = trace_dtype
         self._compensated = bool(compensated)
         self._velocity_mode = velocity_mode
+        if precision not in ("exact", "fast"):
+            raise ValueError("precision must be 'exact' or 'fast'")
+        self._precision = nat.PREC_EXACT if precision == "exact" else nat.PREC_FAST
         self._config = None
         self._ctx = None
         self._lib = None
@@ -155,6 +162,7 @@ class CudaKernel:
         p.curved_k = float(getattr(cfg, "curved_ray_k", 0.5))
         p.eta_constant = float(getattr(cfg, "vti_eta_constant", 0.0))
         p.compensated = int(self._compensated)
+        p.precision = self._precision
         eta = eta_override if eta_override is not None else getattr(cfg, "vti_eta_array", None)
         if eta is not None and tt in (nat.TT_VTI, nat.TT_CURVED_VTI):
             ptr, _ = self._arr(eta, np.float64, keep)
@@ -205,7 +213,8 @@ class CudaKernel:
         if a.ndim != 2 or a.strides[1] != a.itemsize:
             a = np.ascontiguousarray(a)
         keep.append(a)
-        return a.ctypes.data, code, a.strides[0] // a.itemsize, False
+        stride = a.strides[0] // a.itemsize if a.shape[0] > 1 else a.shape[1]
+        return a.ctypes.data, code, max(stride, a.shape[1]), False
 
     def _velocity(self, velocity, output, nx, ny, nt, keep: list):
         v = velocity.vrms
@@ -317,7 +326,7 @@ class CudaKernel:
             raise ValueError("mixing device tensors and host arrays in one call is not supported")
         if on_dev:
             import torch   # order the launch after the producers of the caller's tensors
-            stream = torch.cuda.current_stream().cuda_stream
+            stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
             rc = self._lib.pstm_cuda_migrate_tile_dev(self._ctx, ctypes.byref(td), ctypes.byref(od),
                                                       ctypes.byref(vd), ctypes.byref(prm),
                                                       ctypes.c_void_p(stream))

@@ -1,8 +1,9 @@
 """CUDA backend vs the reference's outputs and the FP64 oracle (GPU).
 
 Tolerances (written here, checked below):
-* plain straight-ray, FP32 traces, vs the reference Numba path: fold
-  bit-exact, image relative L2 <= 1e-5;
+* plain straight-ray, FP32 traces (FP64 sample index, the default), vs the
+  reference Numba path: fold bit-exact, image relative L2 <= 1e-5;
+* the precision form (FP32 traveltime, "fast"): <= 1e-3 against the FP64 oracle;
 * curved / VTI / curved+VTI / AA / 3-D velocity, FP32 traces, vs the FP64
   oracle: fold bit-exact, image relative L2 <= 1e-4;
 * BF16 / FP16 traces: <= 1e-5 against the oracle fed the same rounded traces,
@@ -130,12 +131,13 @@ def test_curved_zero_gradient_and_constant_eta(cuda_kernel_factory):
     assert rel_l2(out.image, ref.image) <= EXACT_KIND_TOL
 
 
+@pytest.mark.parametrize("precision", ["exact", "fast"])
 @pytest.mark.parametrize("dtype", ["bf16", "f16"])
-def test_16bit_traces(dtype, cuda_kernel_factory):
+def test_16bit_traces(dtype, precision, cuda_kernel_factory):
     from pstm_b200 import workloads
     from pstm_b200.cuda_kernel import bf16_bits_to_float32, float32_to_bf16_bits
     case = workloads.config2_small()
-    k = cuda_kernel_factory(case.config, trace_dtype=dtype)
+    k = cuda_kernel_factory(case.config, trace_dtype=dtype, precision=precision)
     k.migrate_tile(case.traces, case.output, case.velocity)
     tb = case.traces
     q = bf16_bits_to_float32(float32_to_bf16_bits(tb.amplitudes)) if dtype == "bf16" \
@@ -145,8 +147,20 @@ def test_16bit_traces(dtype, cuda_kernel_factory):
     ref_q = oracle_run(tq, case.output, case.velocity, case.config)
     ref = oracle_run(tb, case.output, case.velocity, case.config)
     np.testing.assert_array_equal(case.output.fold, ref.fold)
-    assert rel_l2(case.output.image, ref_q.image) <= PLAIN_TOL
+    if precision == "exact":
+        assert rel_l2(case.output.image, ref_q.image) <= PLAIN_TOL
     assert rel_l2(case.output.image, ref.image) <= BF16_TOL
+
+
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p)[6:-4])
+def test_fast_precision_form_on_golden(path, cuda_kernel_factory):
+    """FP32 traveltime (the precision form) against the reference outputs."""
+    tb, out, vel, cfg, img_ref, fold_ref = load_golden_case(path)
+    k = cuda_kernel_factory(cfg, precision="fast")
+    k.migrate_tile(tb, out, vel)
+    np.testing.assert_array_equal(out.fold, fold_ref)
+    if np.abs(img_ref).max() > 0:
+        assert rel_l2(out.image, img_ref) <= BF16_TOL
 
 
 def test_edge_shapes_rotated_grid_f32_image_2d_fold(cuda_kernel_factory):
