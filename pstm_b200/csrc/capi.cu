@@ -14,8 +14,10 @@
 
 namespace pstm {
 template <int TT>
-cudaError_t launch_migrate_tt(const KParams &, const KParams *, int, bool, bool, bool, const TileShape &, dim3,
-                              size_t, cudaStream_t);
+cudaError_t launch_migrate(const KParams &, const KParams *, int, bool, bool, dim3, size_t, cudaStream_t);
+__global__ void pack_geometry(const KParams P, double *geo);
+__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
+                                double *ttimeA);
 }  // namespace pstm
 
 using namespace pstm;
@@ -31,10 +33,11 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    DevBuf ttab, btab, kparams, errword;
+    DevBuf ttab, btab, ttime, ttimeA, kparams, errword, packed_geo;
     // staging for the host-pointer path
     DevBuf amps, geo[7], xa, ya, xg, yg, ta, vel, eta, image, fold;
-    TileShape shape{2, 4};
+    int force_r = 0;      // PSTM_CUDA_R override of the output times per lane
+    int force_pb = 0;     // PSTM_CUDA_PB override of the pillars per CTA
     int smem_optin = 0;   // max dynamic shared memory per block
 };
 
@@ -123,7 +126,7 @@ int32_t validate(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out
 }
 
 KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
-                    const pstm_params *prm, const TileShape &sh) {
+                    const pstm_params *prm, int PB) {
     KParams P;
     std::memset(&P, 0, sizeof(P));
     P.amps = tr->amplitudes;
@@ -147,6 +150,7 @@ KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, con
     P.s_rej_hi = smax + g;
     P.s_max_clamp = std::nextafter(smax, 0.0f);
     P.s_magic = 2147483648.0 - P.tstart_s / P.dt_s;
+    P.inv_dt_f = (float)(1.0 / P.dt_s);
 
     P.image = out->image;
     P.fold = out->fold;
@@ -185,7 +189,6 @@ KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, con
     P.compensated = prm->compensated ? 1 : 0;
 
     // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)
-    const int PB = sh.PBG * kWarpsP;
     int py = PB, px = 1;
     while (py > 1 && py > out->ny) { py /= 2; px *= 2; }
     if (py == PB && PB >= 4) { py = PB / 2; px = 2; }
@@ -202,7 +205,13 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     if (injected("migrate")) return fail(c, PSTM_ERR_INJECTED, "injected fault: migrate");
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
-    KParams P = make_params(tr, out, vel, prm, c->shape);
+    // output times per lane: the whole output trace in one CTA where it fits
+    int R = (out->nt + kThreads - 1) / kThreads;
+    if (R > 8) R = 8;
+    if (c->force_r >= 1 && c->force_r <= 8) R = c->force_r;
+    int PB = R <= 1 ? 8 : 4;
+    if (c->force_pb >= 1 && c->force_pb <= kMaxPB) PB = c->force_pb;
+    KParams P = make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // nothing to add: image += 0, fold += 0
 
     const bool per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
@@ -210,22 +219,41 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     const size_t n_tab = (size_t)n_p * out->nt;
     if ((e = ensure(c->ttab, n_tab * sizeof(float4))) != cudaSuccess ||
         (e = ensure(c->btab, n_tab * sizeof(double))) != cudaSuccess ||
+        (e = ensure(c->ttime, (size_t)out->nt * 2 * sizeof(float4))) != cudaSuccess ||
+        (e = ensure(c->ttimeA, (size_t)out->nt * sizeof(double))) != cudaSuccess ||
         (e = ensure(c->errword, sizeof(int32_t))) != cudaSuccess)
         return cuda_fail(c, e, "allocating the per-time tables");
     float4 *tab = reinterpret_cast<float4 *>(c->ttab.ptr);
     double *btab = reinterpret_cast<double *>(c->btab.ptr);
+    const bool exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
+    P.exact_units = exact ? 1 : 0;
+    P.curved_kind = (prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) ? 1 : 0;
     {
         int blocks = (int)(((int64_t)n_tab + 255) / 256);
         if (blocks > 148 * 32) blocks = 148 * 32;
-        prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab, btab);
+        prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab, btab, reinterpret_cast<float4 *>(c->ttime.ptr),
+                                                reinterpret_cast<double *>(c->ttimeA.ptr));
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(c, e, "prep_time_table launch");
     }
+    P.ttime = reinterpret_cast<const float4 *>(c->ttime.ptr);
+    P.ttimeA = reinterpret_cast<const double *>(c->ttimeA.ptr);
     P.ttab = tab;
     P.btab = btab;
     P.err = reinterpret_cast<int32_t *>(c->errword.ptr);
     if ((e = cudaMemsetAsync(P.err, 0, sizeof(int32_t), st)) != cudaSuccess)
         return cuda_fail(c, e, "clearing the error word");
+
+    // packed FP64 geometry, staged per chunk by TMA bulk copies
+    if ((e = ensure(c->packed_geo, (size_t)tr->n_traces * kGeoDoubles * sizeof(double))) != cudaSuccess)
+        return cuda_fail(c, e, "allocating the packed geometry");
+    {
+        int blocks = (int)((tr->n_traces + 255) / 256);
+        if (blocks > 148 * 32) blocks = 148 * 32;
+        pack_geometry<<<blocks, 256, 0, st>>>(P, reinterpret_cast<double *>(c->packed_geo.ptr));
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(c, e, "pack_geometry launch");
+    }
+    P.geo = reinterpret_cast<const double *>(c->packed_geo.ptr);
 
     // shared-memory staging of trace rows: pitch rounded up to 16 bytes; TMA
     // bulk copies when the rows are 16-byte aligned and the padded row is
@@ -236,19 +264,19 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     const bool aligned = ((uintptr_t)tr->amplitudes % 16 == 0) && ((tr->amp_row_stride * eb) % 16 == 0);
     P.pitch = pitch;
     P.bulk = (aligned && tr->amp_row_stride >= pitch) ? 1 : 0;
-    const TileShape &sh = c->shape;
-    const int PB = sh.PBG * kWarpsP;
-    const bool exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
-    const int nrec = prm->traveltime == PSTM_TT_CURVED_VTI ? 3
-                     : (prm->traveltime == PSTM_TT_STRAIGHT && !prm->aa_enabled) ? 1 : 2;
-    const size_t rec_bytes = (size_t)records_bytes(PB, nrec, exact);
-    const size_t static_bytes = 2048;   // s_ox/s_oy/s_pid/s_fold/barriers, rounded up
-    const size_t budget = (size_t)c->smem_optin > rec_bytes + static_bytes ? c->smem_optin - rec_bytes - static_bytes : 0;
+    const bool has_c = prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI;
+    const size_t fixed = 2 * (size_t)geo_buffer_bytes() + 2 * (size_t)record_buffer_bytes(PB, has_c) +
+                         (size_t)partial_bytes(PB, R);
+    const size_t static_bytes = 3072;   // s_ox/s_oy/s_pid/s_fold/s_rank/barriers, rounded up
+    const size_t budget = (size_t)c->smem_optin > fixed + static_bytes ? c->smem_optin - fixed - static_bytes : 0;
     int chunk = (int)(budget / (2 * (size_t)pitch * eb));
     if (chunk > kMaxChunk) chunk = kMaxChunk;
     if (chunk < 1) return fail(c, PSTM_ERR_UNSUPPORTED, "trace rows too long to stage in shared memory");
     P.chunk = chunk;
-    const size_t smem = 2 * (size_t)chunk * pitch * eb + rec_bytes;
+    P.pb = PB;
+    P.r_per_lane = R;
+    P.flush_every = 16;
+    const size_t smem = 2 * (size_t)chunk * pitch * eb + fixed;
 
     // a device copy of the launch parameters for the kernel's rare FP64 paths
     e = ensure(c->kparams, sizeof(KParams));
@@ -259,16 +287,16 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
 
     const int n_pblk_x = (out->nx + P.px - 1) / P.px;
     const int64_t nblk_p = (int64_t)n_pblk_x * P.n_pblk_y;
-    const int tb = kWarpsT * 32 * sh.R;
+    const int tb = kThreads * R;
     const int nblk_t = (out->nt + tb - 1) / tb;
     if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(c, PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
     dim3 grid((unsigned)nblk_p, (unsigned)nblk_t);
-    const bool aa = prm->aa_enabled != 0;
+    const int amp = tr->amp_dtype;
     switch (prm->traveltime) {
-    case PSTM_TT_STRAIGHT: e = launch_migrate_tt<TT_STRAIGHT>(P, Pg, tr->amp_dtype, per_pillar, aa, exact, sh, grid, smem, st); break;
-    case PSTM_TT_CURVED: e = launch_migrate_tt<TT_CURVED>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
-    case PSTM_TT_VTI: e = launch_migrate_tt<TT_VTI>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
-    default: e = launch_migrate_tt<TT_CURVED_VTI>(P, Pg, tr->amp_dtype, per_pillar, aa, false, sh, grid, smem, st); break;
+    case PSTM_TT_STRAIGHT: e = launch_migrate<TT_STRAIGHT>(P, Pg, amp, per_pillar, exact, grid, smem, st); break;
+    case PSTM_TT_CURVED: e = launch_migrate<TT_CURVED>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
+    case PSTM_TT_VTI: e = launch_migrate<TT_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
+    default: e = launch_migrate<TT_CURVED_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "migrate kernel launch");
     return PSTM_OK;
@@ -327,11 +355,10 @@ int32_t pstm_cuda_create(int32_t device, void **ctx_out) {
         delete c;
         return cuda_fail(nullptr, e, "cudaDeviceGetAttribute");
     }
-    const char *shape = std::getenv("PSTM_CUDA_TILE");   // "R,PBG" override
-    if (shape) {
-        int r, pbg;
-        if (std::sscanf(shape, "%d,%d", &r, &pbg) == 2) c->shape = TileShape{r, pbg};
-    }
+    const char *rr = std::getenv("PSTM_CUDA_R");   // output times per lane override (1..4)
+    if (rr) c->force_r = std::atoi(rr);
+    const char *pb = std::getenv("PSTM_CUDA_PB");   // pillars per CTA override (1..16)
+    if (pb) c->force_pb = std::atoi(pb);
     *ctx_out = c;
     return PSTM_OK;
 }
@@ -343,8 +370,11 @@ void pstm_cuda_destroy(void *ctx) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     release(c->ttab);
     release(c->btab);
+    release(c->ttime);
+    release(c->ttimeA);
     release(c->kparams);
     release(c->errword);
+    release(c->packed_geo);
     release(c->amps);
     for (auto &g : c->geo) release(g);
     release(c->xa); release(c->ya); release(c->xg); release(c->yg); release(c->ta);

@@ -20,6 +20,7 @@ struct KParams {
     int32_t ns;                  // samples per trace
     int32_t elem;                // bytes per amplitude
     const double *sx, *sy, *rx, *ry, *mx, *my, *w;   // w nullable
+    const double *geo;           // packed per trace: sx sy rx ry mx my w 0 (scratch)
     double dt_s, tstart_s;       // input sampling (seconds)
     float s_scale, s_offset;     // sample index s = T * s_scale + s_offset
     float s_guard_lo, s_guard_hi;  // fast-path accept window for s
@@ -30,6 +31,8 @@ struct KParams {
 
     // ---- staging of trace rows in shared memory ----
     int32_t chunk;               // traces per chunk (<= kMaxChunk)
+    int32_t pb;                  // pillars per CTA (<= kMaxPB)
+    int32_t r_per_lane;          // output times per lane (R)
     int32_t pitch;               // staged row pitch, elements (multiple of 16 bytes)
     int32_t bulk;                // 1: rows are copied by TMA bulk copies
     int32_t pad2;
@@ -50,6 +53,12 @@ struct KParams {
     int32_t eta3d;
     const float4 *ttab;          // per (pillar|0, t): {1/v^2, aperture, 1/v, eta}
     const double *btab;          // per (pillar|0, t): 1/(v dt)^2 (EXACT path)
+    const float4 *ttime;         // per t: {t0h2, Kt, tg, tguard}, {vz, vz2, 1/vz, t0 == 0}
+    const double *ttimeA;        // per t: (t0 / (2 dt))^2 (EXACT path)
+    float inv_dt_f;              // 1 / dt (s)
+    int32_t flush_every;         // chunks between flushes of the FP32 partials
+    int32_t exact_units;         // weights' time unit: 1 = samples (EXACT), 0 = seconds
+    int32_t curved_kind;         // curved-ray traveltime (its T can be ~0 at t0 > 0)
     const double *eta;           // nullable (FP64, exact paths)
     double eta_const;
 

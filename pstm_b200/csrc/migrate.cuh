@@ -1,19 +1,22 @@
 // migrate.cuh -- gather-form Kirchhoff PSTM kernel for sm_100a.
 //
-// One CTA (16 warps) owns a patch of PB output pillars and a block of
-// kWarpsT * 32 * R consecutive output times.  The warps form kWarpsP pillar
-// groups x kWarpsT time groups; a lane owns R output times (t = base + r*32 +
-// lane) for the PBG = PB / kWarpsP pillars of its group and keeps their sums in
+// One CTA (16 warps, 512 lanes) owns PB output pillars and, for each of them,
+// a block of 512*R output times; lane `tid` owns the R times
+// t = t_block + tid + 512*r, so every warp holds shallow and deep times alike
+// and the work per warp is balanced.  A lane keeps the PB x R partial sums in
 // registers.  Traces are streamed in chunks of C:
-//   staging  the chunk's amplitude rows are copied into shared memory by TMA
-//            bulk copies (cp.async.bulk + mbarrier), double-buffered, so the
-//            copy of chunk k+1 overlaps the arithmetic of chunk k;
-//   phase A  every (pillar, trace) pair of the chunk gets a record in shared
-//            memory (FP64 geometry rounded once to FP32); the fold predicate
-//            is evaluated in FP64 and counted with warp match/ballot + popc;
-//   phase B  every lane walks the records (warp-uniform broadcast reads) and,
-//            for each of its R times, evaluates traveltime, the sample index,
-//            the linear interpolation (from shared memory) and the weights.
+//   staging  the chunk's amplitude rows and packed FP64 geometry are copied
+//            into shared memory by TMA bulk copies (cp.async.bulk + mbarrier),
+//            double-buffered, so chunk k+1 lands while chunk k is processed;
+//   records  every (pillar, trace) pair of the next chunk gets a record in
+//            shared memory (FP64 geometry rounded once to FP32); the fold
+//            predicate is evaluated in FP64 and counted with warp match /
+//            ballot + popc;
+//   pairs    every lane walks the records of the current chunk (warp-uniform
+//            broadcast reads) and, for each of its R times, evaluates
+//            traveltime, sample index, linear interpolation (from shared
+//            memory) and weights, with warp-uniform skips instead of
+//            divergent branches.
 // Chunk partials are folded into compensated (TwoSum) FP32 sums and the
 // epilogue adds them once into the caller's image (+=) and fold.
 //
@@ -28,22 +31,21 @@
 // with a Newton-refined sqrt) and split into integer and fraction with bit
 // operations, so the interpolation position carries ~2^-21 samples of error
 // and the trace-end test is an FP64 decision.  Otherwise traveltime is FP32
-// and decisions that are discontinuous in the inputs (aperture cut, trace-end
-// bounds) are re-taken in FP64 inside a guard band.
+// and the trace-end decision is re-taken in FP64 inside a guard band.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
+#include <type_traits>
 #include "kparams.h"
 
 namespace pstm {
 
-constexpr int kWarpsT = 8;                         // warps along time
-constexpr int kWarpsP = 2;                         // warp groups along pillars
-constexpr int kThreads = 32 * kWarpsT * kWarpsP;   // 512
-constexpr int kMaxChunk = 32;                      // traces per chunk, upper bound
-constexpr int kWaitIters = 1 << 20;                // bound of every mbarrier wait loop
+constexpr int kThreads = 512;        // lanes per CTA = output times per r
+constexpr int kMaxChunk = 32;        // traces per chunk, upper bound
+constexpr int kGeoDoubles = 8;       // packed geometry per trace: sx sy rx ry mx my w 0
+constexpr int kWaitIters = 1 << 20;  // bound of every mbarrier wait loop
 
 // ---------------------------------------------------------------- math helpers
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -120,61 +122,50 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 }
 
 // ---------------------------------------------------------------- per-time state
-// Quantities that depend on the output time only (one copy per lane and r).
+// Quantities that depend on the output time only: one table entry per time
+// (prep_time_table), loaded per (pillar, r) just before the record loop.
 struct TimeState {
-    float t0, t0h2;
+    float t0h2;
     float Kt;              // obliquity numerator t0 (in the weight's time unit) or 1
-    float tguard;          // T <= tguard means "T <= 1 ms" (in the unit of T)
+    float tg;              // weights apply only when T > tg ("T > 1 ms"); -1 when always
+    float tguard;          // 1 ms in the unit of T
     float vz, vz2, ivwc;   // curved: velocity at image depth, 1/vz
-    double A;              // EXACT: (t0 / (2 dt))^2
-    bool valid, guard, tzero;
+    bool tzero;
+    double A;              // EXACT: (t0 / (2 dt))^2 (at least 1e-300)
 };
 
-// Quantities that depend on (pillar, time): from the per-pillar tables.
+// Quantities that depend on (pillar, time).
 struct PtState {
     float iv2, ap, itw, tsn;
     float K;               // weight numerator
-    float ivw_t;           // 1/v_w in the weight's time unit (AA sin theta)
-    float ivw;             // 1/v_w in s/m (AA f_max)
+    float ivw_t;           // 1/v_w per unit of T (AA sin theta)
+    float aaA;             // 4 max(dx,dy) f_dom / v_w (AA)
     float t02v2, c1, e2;   // VTI: (t0/2)^2 v^2, 1+2eta, 2 eta / v^2
     double B;              // EXACT: 1/(v dt)^2
 };
 
 template <int TT, bool EXACT>
-__device__ __forceinline__ void make_time_state(const KParams &P, int t, TimeState &s) {
-    s.valid = t < P.nt;
-    const int tc = s.valid ? t : (P.nt - 1);
-    const double t0 = P.ta[tc] / 1000.0;
-    const double tu = EXACT ? P.dt_s : 1.0;   // weights' time unit: seconds, or samples
-    s.t0 = (float)t0;
-    s.t0h2 = (float)((t0 * 0.5) * (t0 * 0.5));
-    s.Kt = P.obliquity ? (float)(t0 / tu) : 1.f;
-    s.tguard = (float)(0.001 / tu);
-    s.vz = 0.f;
-    s.vz2 = 0.f;
-    s.ivwc = 0.f;
-    if constexpr (TT == TT_CURVED || TT == TT_CURVED_VTI) {
-        const double z = P.cr_k_zero ? P.cr_v0 * (t0 * 0.5) : (P.cr_v0 / P.cr_k) * (exp(P.cr_k * (t0 * 0.5)) - 1.0);
-        const double vz = P.cr_v0 + P.cr_k * z;
-        s.vz = (float)vz;
-        s.vz2 = (float)(vz * vz);
-        s.ivwc = (float)(1.0 / vz);
-    }
-    const double th = t0 * 0.5 / P.dt_s;
-    s.A = EXACT ? th * th : 0.0;
-    s.guard = t0 < 0.0011;
-    s.tzero = !(t0 > 0.0);
-}
-
-template <int TT, bool EXACT>
-__device__ __forceinline__ void make_pt_state(const KParams &P, const TimeState &ts, float4 tab, double b,
-                                              PtState &s) {
+__device__ __forceinline__ void load_states(const KParams &P, int p, int t, TimeState &ts, PtState &s) {
+    const bool valid = t < P.nt;
+    const int tc = valid ? t : P.nt - 1;
+    const float4 a = P.ttime[2 * tc], b = P.ttime[2 * tc + 1];
+    ts.t0h2 = a.x;
+    ts.Kt = a.y;
+    ts.tg = a.z;
+    ts.tguard = a.w;
+    ts.vz = b.x;
+    ts.vz2 = b.y;
+    ts.ivwc = b.z;
+    ts.tzero = b.w != 0.f;
+    ts.A = EXACT ? P.ttimeA[tc] : 0.0;
+    const int64_t ti = (P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc;
+    const float4 tab = P.ttab[ti];
     s.iv2 = tab.x;
-    s.ap = tab.y;
-    const float width = s.ap * P.taper_f;
+    s.ap = valid ? tab.y : -1.f;   // a time past the tile end is never inside the aperture
+    const float width = tab.y * P.taper_f;
     if (width > 0.f) {
         s.itw = rcp_approx(width);
-        s.tsn = -(s.ap * (1.f - P.taper_f)) * s.itw;
+        s.tsn = -(tab.y * (1.f - P.taper_f)) * s.itw;
     } else {
         s.itw = 0.f;
         s.tsn = -1.f;
@@ -186,9 +177,8 @@ __device__ __forceinline__ void make_pt_state(const KParams &P, const TimeState 
         if (P.cr_k_zero) s.iv2 = ts.ivwc * ts.ivwc;
     }
     // T is in seconds, or in samples on the EXACT path: 1/(v T_sec) = (1/(v dt)) / T_samples
-    const float inv_tu = EXACT ? (float)(1.0 / P.dt_s) : 1.f;
-    s.ivw = ivw;
-    s.ivw_t = ivw * inv_tu;
+    s.ivw_t = EXACT ? ivw * P.inv_dt_f : ivw;
+    s.aaA = P.aa_cA * ivw;
     s.K = P.spreading ? ts.Kt * s.ivw_t : ts.Kt;
     s.t02v2 = 0.f;
     s.c1 = 1.f;
@@ -198,7 +188,22 @@ __device__ __forceinline__ void make_pt_state(const KParams &P, const TimeState 
         s.c1 = 1.f + 2.f * tab.w;
         s.e2 = 2.f * tab.w * tab.x;
     }
-    s.B = b;
+    s.B = EXACT ? P.btab[ti] : 0.0;
+}
+
+// 0.5 (1 + cos(pi x)) = cos^2(pi x / 2) for x in [0, 1]: Taylor series of cos
+// about 0 through y^12 (|error| < 7e-9 on y in [0, pi/2]), then squared.
+__device__ __forceinline__ float taper_weight(float x) {
+    const float y = 1.57079632679489662f * x;
+    const float u = y * y;
+    float c = 2.08767569878681e-9f;                 //  1/12!
+    c = fmaf(c, u, -2.75573192239859e-7f);          // -1/10!
+    c = fmaf(c, u, 2.48015873015873e-5f);           //  1/8!
+    c = fmaf(c, u, -1.38888888888889e-3f);          // -1/6!
+    c = fmaf(c, u, 4.16666666666667e-2f);           //  1/4!
+    c = fmaf(c, u, -0.5f);                          // -1/2!
+    c = fmaf(c, u, 1.0f);
+    return c * c;
 }
 
 // ---------------------------------------------------------------- FP64 exact decisions
@@ -276,80 +281,91 @@ static __device__ __noinline__ bool exact_outside_aperture(const KParams *P, int
 }
 
 // ---------------------------------------------------------------- traveltime (FP32)
-// rec0 = {ds2, dr2, d, wt}; rec1/rec2 kind-specific (see phase A).  Seconds.
+// Records: A = {d, wt, minf, trace slot}; B = {ds2, dr2, k^2 ds2 | ds2^2, k^2 dr2 | dr2^2};
+// C (curved kinds) = {1/(bs br) | 1/bs, 1/br, ds2^2, dr2^2}.  Result in seconds.
 template <int TT>
 __device__ __forceinline__ float traveltime(const KParams &P, const TimeState &ts, const PtState &s,
-                                            const float4 &r0, const float4 &r1, const float4 &r2) {
+                                            const float4 &B, const float4 &Cc) {
     if constexpr (TT == TT_STRAIGHT) {
-        return sqrt_approx(fmaf(r0.x, s.iv2, ts.t0h2)) + sqrt_approx(fmaf(r0.y, s.iv2, ts.t0h2));
+        return sqrt_approx(fmaf(B.x, s.iv2, ts.t0h2)) + sqrt_approx(fmaf(B.y, s.iv2, ts.t0h2));
     } else if constexpr (TT == TT_CURVED) {
         if (P.cr_k_zero) {
-            return sqrt_approx(fmaf(r0.x, s.iv2, ts.t0h2)) + sqrt_approx(fmaf(r0.y, s.iv2, ts.t0h2));
+            return sqrt_approx(fmaf(B.x, s.iv2, ts.t0h2)) + sqrt_approx(fmaf(B.y, s.iv2, ts.t0h2));
         }
-        const float a = ts.vz + sqrt_approx(ts.vz2 + r1.y);
-        const float b = ts.vz + sqrt_approx(ts.vz2 + r1.z);
-        return P.cr_inv_k_ln2 * lg2_approx(a * b * r1.w);
+        const float a = ts.vz + sqrt_approx(ts.vz2 + B.z);
+        const float b = ts.vz + sqrt_approx(ts.vz2 + B.w);
+        return P.cr_inv_k_ln2 * lg2_approx(a * b * Cc.x);
     } else if constexpr (TT == TT_VTI) {
         if (ts.tzero) return 0.f;
-        const float Ds = fmaf(s.c1, r0.x, s.t02v2);
-        const float Dr = fmaf(s.c1, r0.y, s.t02v2);
+        const float Ds = fmaf(s.c1, B.x, s.t02v2);
+        const float Dr = fmaf(s.c1, B.y, s.t02v2);
         const float rr = rcp_approx(Ds * Dr);
-        const float qs = fmaf(-(s.e2 * r1.y), Dr * rr, fmaf(r0.x, s.iv2, ts.t0h2));
-        const float qr = fmaf(-(s.e2 * r1.z), Ds * rr, fmaf(r0.y, s.iv2, ts.t0h2));
+        const float qs = fmaf(-(s.e2 * B.z), Dr * rr, fmaf(B.x, s.iv2, ts.t0h2));
+        const float qr = fmaf(-(s.e2 * B.w), Ds * rr, fmaf(B.y, s.iv2, ts.t0h2));
         return sqrt_approx(fmaxf(qs, 0.f)) + sqrt_approx(fmaxf(qr, 0.f));
     } else {
         float tcs, tcr;
         if (P.cr_k_zero) {
-            tcs = sqrt_approx(fmaf(r0.x, s.iv2, ts.t0h2));
-            tcr = sqrt_approx(fmaf(r0.y, s.iv2, ts.t0h2));
+            tcs = sqrt_approx(fmaf(B.x, s.iv2, ts.t0h2));
+            tcr = sqrt_approx(fmaf(B.y, s.iv2, ts.t0h2));
         } else {
-            const float a = ts.vz + sqrt_approx(ts.vz2 + r1.y);
-            const float b = ts.vz + sqrt_approx(ts.vz2 + r1.z);
-            tcs = P.cr_inv_k_ln2 * lg2_approx(a * r1.w);
-            tcr = P.cr_inv_k_ln2 * lg2_approx(b * r2.x);
+            const float a = ts.vz + sqrt_approx(ts.vz2 + B.z);
+            const float b = ts.vz + sqrt_approx(ts.vz2 + B.w);
+            tcs = P.cr_inv_k_ln2 * lg2_approx(a * Cc.x);
+            tcr = P.cr_inv_k_ln2 * lg2_approx(b * Cc.y);
         }
         if (ts.tzero) return tcs + tcr;
         // leg = t_curved * sqrt(1 - corr / (t0h^2 + h^2/v^2)), corr = e2 h^4 / D
-        const float Hs = fmaf(r0.x, s.iv2, ts.t0h2), Hr = fmaf(r0.y, s.iv2, ts.t0h2);
-        const float Ds = fmaf(s.c1, r0.x, s.t02v2), Dr = fmaf(s.c1, r0.y, s.t02v2);
+        const float Hs = fmaf(B.x, s.iv2, ts.t0h2), Hr = fmaf(B.y, s.iv2, ts.t0h2);
+        const float Ds = fmaf(s.c1, B.x, s.t02v2), Dr = fmaf(s.c1, B.y, s.t02v2);
         const float ps_ = Ds * Hs, pr_ = Dr * Hr;
         const float rr = rcp_approx(ps_ * pr_);
-        const float xs = s.e2 * r2.y * (pr_ * rr), xr = s.e2 * r2.z * (ps_ * rr);
+        const float xs = s.e2 * Cc.z * (pr_ * rr), xr = s.e2 * Cc.w * (ps_ * rr);
         return tcs * sqrt_approx(fmaxf(1.f - xs, 0.f)) + tcr * sqrt_approx(fmaxf(1.f - xr, 0.f));
     }
 }
 
-template <int TT, bool AA>
-struct RecCount {
-    static constexpr int value = (TT == TT_CURVED_VTI) ? 3 : ((TT == TT_STRAIGHT && !AA) ? 1 : 2);
+template <int TT>
+struct RecLayout {
+    static constexpr bool kHasC = (TT == TT_CURVED || TT == TT_CURVED_VTI);
 };
 
-// Record area of the dynamic shared memory (after the two staging buffers).
-__host__ __device__ constexpr int records_bytes(int PB, int nrec, bool exact) {
-    return PB * kMaxChunk * (16 * nrec + (exact ? 16 : 0));
+constexpr int kMaxPB = 16;   // pillars per CTA, upper bound (one warp per pillar builds records)
+
+// Bytes of one record buffer (the kernel keeps two): A, B and (curved kinds) C.
+__host__ __device__ constexpr int record_buffer_bytes(int PB, bool has_c) {
+    return PB * kMaxChunk * 16 * (has_c ? 3 : 2);
 }
+__host__ __device__ constexpr int geo_buffer_bytes() { return kMaxChunk * kGeoDoubles * 8; }
+// Per-lane FP32 partial sums of one CTA: PB x R x kThreads floats.
+__host__ __device__ constexpr int partial_bytes(int PB, int R) { return PB * R * kThreads * 4; }
 
 // ---------------------------------------------------------------- the kernel
-template <int TT, int AMP, bool VEL3D, bool AA, bool EXACT, int R, int PBG>
+template <int TT, int AMP, bool VEL3D, bool EXACT>
 __global__ void __launch_bounds__(kThreads, 1)
-migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
+migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
-    constexpr int PB = PBG * kWarpsP;
-    constexpr int NREC = RecCount<TT, AA>::value;
-    constexpr int RECS = PB * kMaxChunk;
+    static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
+    constexpr bool HAS_C = RecLayout<TT>::kHasC;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ double s_ox[PB], s_oy[PB];
-    __shared__ int s_pid[PB];
-    __shared__ int s_fold[PB];
+    __shared__ double s_ox[kMaxPB], s_oy[kMaxPB];
+    __shared__ int s_pid[kMaxPB];
+    __shared__ int s_fold[kMaxPB];
+    __shared__ int s_rank[kMaxPB][kMaxChunk];
     __shared__ __align__(8) unsigned long long s_bar[2];
 
+    const int PB = P.pb, R = P.r_per_lane;
+    const int RECS = PB * kMaxChunk;
+    const int REC_BYTES = record_buffer_bytes(PB, HAS_C);
     const int C = P.chunk;
-    const int buf_bytes = C * P.pitch * P.elem;
-    float4 *s_rec = reinterpret_cast<float4 *>(smem + 2 * buf_bytes);     // [NREC][RECS]
-    double2 *s_rec64 = reinterpret_cast<double2 *>(s_rec + NREC * RECS);  // [RECS] (EXACT)
+    const int row_bytes = P.pitch * P.elem;
+    const int amp_bytes = C * row_bytes;   // multiple of 16
+    unsigned char *const amp_base = smem;
+    unsigned char *const geo_base = smem + 2 * amp_bytes;
+    unsigned char *const rec_base = geo_base + 2 * geo_buffer_bytes();
+    float *const s_acc = reinterpret_cast<float *>(rec_base + 2 * REC_BYTES);   // [PB][R][kThreads]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wp = warp / kWarpsT, wt = warp - wp * kWarpsT;
     const int pbx = blockIdx.x / P.n_pblk_y, pby = blockIdx.x - pbx * P.n_pblk_y;
     if (tid < PB) {
         const int ix = pbx * P.px + tid / P.py, iy = pby * P.py + tid % P.py;
@@ -366,7 +382,7 @@ migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
         mbar_init(bar1, 1);
         fence_barrier_init();
     }
-    const int t_base = blockIdx.y * (kWarpsT * 32 * R) + wt * (32 * R) + lane;
+    const int t_lane = blockIdx.y * (kThreads * R) + tid;
 
     // hot-loop constants in registers
     const float s_scale = P.s_scale, s_offset = P.s_offset;
@@ -374,116 +390,114 @@ migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
     const float s_clamp = P.s_max_clamp;
     const unsigned ns_m1 = (unsigned)(P.ns - 1);
     const double magic = P.s_magic;
-    const float ap_max_f = P.ap_max_f;
-    const int nw = P.spreading + P.obliquity;
-    const float aa_cA = P.aa_cA, aa_cB = P.aa_cB;
-    const int row_bytes = P.pitch * P.elem;
+    const bool w_one = P.spreading + P.obliquity == 1, w_two = P.spreading + P.obliquity == 2;
+    const float aa_cB = P.aa_cB;
+    const bool aa_on = P.aa != 0;
+    const bool hard_cut = !(P.taper_f > 0.f);
+    const float one_m_taper = 1.f - P.taper_f;
     const int64_t n_chunks = (P.n_traces + C - 1) / C;
+    const int flush_every = P.flush_every;
 
-    TimeState ts[R];
-    PtState ps[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) make_time_state<TT, EXACT>(P, t_base + r * 32, ts[r]);
-    if constexpr (!VEL3D) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int t = min(t_base + r * 32, P.nt - 1);
-            make_pt_state<TT, EXACT>(P, ts[r], P.ttab[t], EXACT ? P.btab[t] : 0.0, ps[r]);
-        }
-    }
+    for (int i = tid; i < PB * R * kThreads; i += kThreads) s_acc[i] = 0.f;
 
-    float acc[PBG][R], hi[PBG][R], lo[PBG][R];
-#pragma unroll
-    for (int g = 0; g < PBG; ++g)
-#pragma unroll
-        for (int r = 0; r < R; ++r) { acc[g][r] = 0.f; hi[g][r] = 0.f; lo[g][r] = 0.f; }
-
-    // copy the amplitude rows of chunk k into buffer b (one thread, TMA bulk)
+    // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
+    // rows when they are 16-byte aligned) into buffer b
     auto issue_chunk = [&](int64_t k, int b) {
         const int64_t c0 = k * C;
         const int rows = (int)min((int64_t)C, P.n_traces - c0);
         const uint32_t bar = b ? bar1 : bar0;
-        mbar_expect_tx(bar, (uint32_t)(rows * row_bytes));
-        const unsigned char *src = reinterpret_cast<const unsigned char *>(P.amps) + c0 * P.amp_stride * P.elem;
-        const uint32_t dst = smem_u32(smem + b * buf_bytes);
-        for (int i = 0; i < rows; ++i)
-            bulk_g2s(dst + i * row_bytes, src + (int64_t)i * P.amp_stride * P.elem, (uint32_t)row_bytes, bar);
+        const uint32_t geo_bytes = (uint32_t)(rows * kGeoDoubles * 8);
+        mbar_expect_tx(bar, geo_bytes + (P.bulk ? (uint32_t)(rows * row_bytes) : 0u));
+        bulk_g2s(smem_u32(geo_base + b * geo_buffer_bytes()), P.geo + c0 * kGeoDoubles, geo_bytes, bar);
+        if (P.bulk) {
+            const unsigned char *src = reinterpret_cast<const unsigned char *>(P.amps) + c0 * P.amp_stride * P.elem;
+            const uint32_t dst = smem_u32(amp_base + b * amp_bytes);
+            for (int i = 0; i < rows; ++i)
+                bulk_g2s(dst + i * row_bytes, src + (int64_t)i * P.amp_stride * P.elem, (uint32_t)row_bytes, bar);
+        }
     };
 
-    __syncthreads();
-    if (P.bulk && tid == 0) {
-        issue_chunk(0, 0);
-        if (n_chunks > 1) issue_chunk(1, 1);
-    }
-
-    bool aborted = false;
-    for (int64_t k = 0; k < n_chunks; ++k) {
+    // Records of chunk k from the staged geometry in buffer b: warp q builds
+    // pillar q's 32 records, counts its fold and sorts them by midpoint
+    // distance (bitonic, in registers) so that, for any aperture, the records
+    // inside it form a prefix.
+    auto build_records = [&](int64_t k, int b) {
         const int64_t c0 = k * C;
-        const int buf = (int)(k & 1);
         const int cmax = (int)min((int64_t)C, P.n_traces - c0);
-        // ---------------- phase A: (pillar, trace) records, FP64 geometry
-        const int nrec = PB * C;
-        for (int j = tid; j < ((nrec + 31) & ~31); j += kThreads) {
-            const bool live = j < nrec;
-            const int q = live ? j / C : PB - 1;
-            const int c = live ? j - q * C : 0;
-            const int64_t tr = c0 + c;
+        if (warp < PB) {
+            const int q = warp, c = lane;
+            const double *geo = reinterpret_cast<const double *>(geo_base + b * geo_buffer_bytes());
+            float4 *recA = reinterpret_cast<float4 *>(rec_base + b * REC_BYTES);
             const int p = s_pid[q];
             bool in = false;
-            float4 r0 = make_float4(0.f, 0.f, __int_as_float(0x7f800000), 0.f);
-            float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f), r2 = r1;
-            double2 r64 = make_double2(0.0, 0.0);
-            if (live && p >= 0 && c < cmax) {
+            const float inf = __int_as_float(0x7f800000);
+            float4 A = make_float4(inf, 0.f, 0.f, __int_as_float(c));
+            float4 Bf = make_float4(0.f, 0.f, 0.f, 0.f), Cc = Bf;
+            double2 B64 = make_double2(0.0, 0.0);
+            if (p >= 0 && c < cmax) {
+                const double *g = geo + c * kGeoDoubles;   // sx sy rx ry mx my w
                 const double ox = s_ox[q], oy = s_oy[q];
-                const double dxm = ox - P.mx[tr], dym = oy - P.my[tr];
+                const double dxm = ox - g[4], dym = oy - g[5];
                 const double d2 = dxm * dxm + dym * dym;
                 in = d2 <= P.fold_d2_max;
                 if (in) {
-                    const double dxs = ox - P.sx[tr], dys = oy - P.sy[tr];
-                    const double dxr = ox - P.rx[tr], dyr = oy - P.ry[tr];
+                    const double dxs = ox - g[0], dys = oy - g[1];
+                    const double dxr = ox - g[2], dyr = oy - g[3];
                     const double ds2 = dxs * dxs + dys * dys, dr2 = dxr * dxr + dyr * dyr;
-                    const float wt = P.w ? (float)P.w[tr] : 1.f;
-                    r0 = make_float4((float)ds2, (float)dr2, (float)sqrt(d2), wt);
-                    r64 = make_double2(ds2, dr2);
-                    const float minf = (float)fmax(fabs(dxm), fabs(dym));
+                    // the FP64 sqrt is needed only where the aperture cut is hard
+                    const float d = hard_cut ? (float)sqrt(d2) : sqrt_approx((float)d2);
+                    A = make_float4(d, (float)g[6], (float)fmax(fabs(dxm), fabs(dym)), __int_as_float(c));
+                    B64 = make_double2(ds2, dr2);
+                    Bf = make_float4((float)ds2, (float)dr2, 0.f, 0.f);
                     if constexpr (TT == TT_CURVED || TT == TT_CURVED_VTI) {
                         const double k2 = P.cr_k * P.cr_k, v0 = P.cr_v0;
                         const double bs = v0 + sqrt(v0 * v0 + k2 * ds2);
                         const double br = v0 + sqrt(v0 * v0 + k2 * dr2);
+                        Bf.z = (float)(k2 * ds2);
+                        Bf.w = (float)(k2 * dr2);
                         if constexpr (TT == TT_CURVED) {
-                            r1 = make_float4(minf, (float)(k2 * ds2), (float)(k2 * dr2), (float)(1.0 / (bs * br)));
+                            Cc = make_float4((float)(1.0 / (bs * br)), 0.f, 0.f, 0.f);
                         } else {
-                            r1 = make_float4(minf, (float)(k2 * ds2), (float)(k2 * dr2), (float)(1.0 / bs));
-                            r2 = make_float4((float)(1.0 / br), (float)(ds2 * ds2), (float)(dr2 * dr2), 0.f);
+                            Cc = make_float4((float)(1.0 / bs), (float)(1.0 / br), (float)(ds2 * ds2),
+                                             (float)(dr2 * dr2));
                         }
                     } else if constexpr (TT == TT_VTI) {
-                        r1 = make_float4(minf, (float)(ds2 * ds2), (float)(dr2 * dr2), 0.f);
-                    } else {
-                        r1 = make_float4(minf, 0.f, 0.f, 0.f);
+                        Bf.z = (float)(ds2 * ds2);
+                        Bf.w = (float)(dr2 * dr2);
                     }
                 }
             }
-            // fold: lanes with the same pillar share one shared-memory add
-            const unsigned peers = __match_any_sync(0xffffffffu, q);
             const unsigned ballot = __ballot_sync(0xffffffffu, in);
-            if (lane == __ffs(peers) - 1) {
-                const int cnt = __popc(ballot & peers);
-                if (cnt) atomicAdd(&s_fold[q], cnt);
+            if (lane == 0) s_fold[q] += __popc(ballot);
+            // bitonic sort of (d, lane) ascending across the warp
+            float key = A.x;
+            int idx = lane;
+#pragma unroll
+            for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+                for (int j = kk >> 1; j > 0; j >>= 1) {
+                    const float ok_ = __shfl_xor_sync(0xffffffffu, key, j);
+                    const int oi = __shfl_xor_sync(0xffffffffu, idx, j);
+                    const bool up = (lane & kk) == 0, lower = (lane & j) == 0;
+                    const bool other_less = ok_ < key || (ok_ == key && oi < idx);
+                    const bool take = (lower == up) ? other_less : !other_less;
+                    key = take ? ok_ : key;
+                    idx = take ? oi : idx;
+                }
             }
-            if (live) {
-                const int ri = q * kMaxChunk + c;
-                s_rec[ri] = r0;
-                if constexpr (NREC > 1) s_rec[RECS + ri] = r1;
-                if constexpr (NREC > 2) s_rec[2 * RECS + ri] = r2;
-                if constexpr (EXACT) s_rec64[ri] = r64;
-            }
+            s_rank[q][idx] = lane;   // lane L holds the L-th smallest: idx goes to slot L
+            __syncwarp();
+            const int ri = q * kMaxChunk + s_rank[q][lane];
+            recA[ri] = A;
+            if constexpr (EXACT) reinterpret_cast<double2 *>(recA + RECS)[ri] = B64;
+            else reinterpret_cast<float4 *>(recA + RECS)[ri] = Bf;
+            if constexpr (HAS_C) reinterpret_cast<float4 *>(recA + 2 * RECS)[ri] = Cc;
         }
-        if (!P.bulk) {   // rows not 16-byte aligned: plain cooperative copy
-            unsigned char *dst = smem + buf * buf_bytes;
+        if (!P.bulk) {   // amplitude rows not 16-byte aligned: plain cooperative copy
+            unsigned char *dst = amp_base + b * amp_bytes;
             const unsigned char *src = reinterpret_cast<const unsigned char *>(P.amps);
-            const int per_row = P.ns;
-            for (int e = tid; e < cmax * per_row; e += kThreads) {
-                const int rr = e / per_row, ii = e - rr * per_row;
+            for (int e = tid; e < cmax * P.ns; e += kThreads) {
+                const int rr = e / P.ns, ii = e - rr * P.ns;
                 const int64_t gi = (c0 + rr) * P.amp_stride + ii;
                 if (P.elem == 4)
                     reinterpret_cast<float *>(dst + rr * row_bytes)[ii] = reinterpret_cast<const float *>(src)[gi];
@@ -492,129 +506,167 @@ migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
                         reinterpret_cast<const unsigned short *>(src)[gi];
             }
         }
-        __syncthreads();
-        if (P.bulk) {
-            const bool ok = mbar_wait(buf ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
-            if (__syncthreads_or(!ok)) {
-                aborted = true;
-                break;
+    };
+
+    // add this lane's FP32 partial sums into the FP64 (or FP32) image and clear them
+    auto flush = [&]() {
+#pragma unroll 1
+        for (int q = 0; q < PB; ++q) {
+            const int p = s_pid[q];
+#pragma unroll 1
+            for (int r = 0; r < R; ++r) {
+                const int t = t_lane + r * kThreads;
+                float &a = s_acc[(q * R + r) * kThreads + tid];
+                if (p >= 0 && t < P.nt && a != 0.f) {
+                    const int64_t idx = (int64_t)p * P.nt + t;
+                    if (P.image_f32) reinterpret_cast<float *>(P.image)[idx] += a;
+                    else reinterpret_cast<double *>(P.image)[idx] += (double)a;
+                }
+                a = 0.f;
             }
         }
+    };
 
-        // ---------------- phase B: pairs
-        const unsigned char *bufp = smem + buf * buf_bytes;
-#pragma unroll
-        for (int g = 0; g < PBG; ++g) {
-            const int q = wp * PBG + g;
+    __syncthreads();   // barriers initialised, pillars known
+    if (tid == 0) {
+        if (n_chunks > 0) issue_chunk(0, 0);
+        if (n_chunks > 1) issue_chunk(1, 1);
+    }
+    bool aborted = false;
+    if (n_chunks > 0) {
+        const bool ok = mbar_wait(bar0, 0);
+        if (__syncthreads_or(!ok)) aborted = true;
+        else build_records(0, 0);
+    }
+    __syncthreads();
+
+    for (int64_t k = 0; k < n_chunks && !aborted; ++k) {
+        const int64_t c0 = k * C;
+        const int buf = (int)(k & 1);
+        const float4 *recA = reinterpret_cast<const float4 *>(rec_base + buf * REC_BYTES);
+        const unsigned char *ampb = amp_base + buf * amp_bytes;
+
+        // ---------------- pairs of chunk k
+#pragma unroll 1
+        for (int q = 0; q < PB; ++q) {
             const int p = s_pid[q];
             if (p < 0) continue;
-            if constexpr (VEL3D) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const int64_t ti = (int64_t)p * P.nt + min(t_base + r * 32, P.nt - 1);
-                    make_pt_state<TT, EXACT>(P, ts[r], P.ttab[ti], EXACT ? P.btab[ti] : 0.0, ps[r]);
-                }
-            }
-#pragma unroll 2
-            for (int c = 0; c < cmax; ++c) {
-                const int ri = q * kMaxChunk + c;
-                const float4 r0 = s_rec[ri];
-                if (!(r0.z <= ap_max_f)) continue;
-                float4 r1 = make_float4(0.f, 0.f, 0.f, 0.f), r2 = r1;
-                if constexpr (NREC > 1) r1 = s_rec[RECS + ri];
-                if constexpr (NREC > 2) r2 = s_rec[2 * RECS + ri];
-                double2 r64 = make_double2(0.0, 0.0);
-                if constexpr (EXACT) r64 = s_rec64[ri];
-                const unsigned char *row = bufp + c * row_bytes;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    const TimeState &t_ = ts[r];
-                    const PtState &s = ps[r];
-                    if (!t_.valid) continue;
-                    if (r0.z >= s.ap) {
-                        if (r0.z > s.ap) continue;
-                        if (exact_outside_aperture(Pg, c0 + c, p, t_base + r * 32, s_ox[q], s_oy[q])) continue;
-                    }
+            const float4 *A_q = recA + q * kMaxChunk;
+            const float dl = A_q[lane].x;   // this lane's slot of the sorted distances
+#pragma unroll 1
+            for (int r = 0; r < R; ++r) {
+                const int t = t_lane + r * kThreads;
+                TimeState ts;
+                PtState s;
+                load_states<TT, EXACT>(P, p, t, ts, s);
+                // records inside the aperture of some lane: a prefix of length n;
+                // records with no lane in its taper band: a prefix of length n0
+                const float apw = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(s.ap)));
+                const float tsl = s.ap > 0.f ? s.ap * one_m_taper : __int_as_float(0x7f800000);
+                const float tmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(tsl)));
+                const int n = __popc(__ballot_sync(0xffffffffu, dl <= apw));
+                const int n0 = min(n, __popc(__ballot_sync(0xffffffffu, dl <= tmin)));
+                bool pend = false;   // FP32 path: some pair lies in a trace-end guard band
+
+                // contribution of record c (slot in the sorted order) to this lane's time
+                auto pair = [&](int c, auto taper_c, auto slow_c) -> float {
+                    constexpr bool TAPER = decltype(taper_c)::value;
+                    constexpr bool SLOW = decltype(slow_c)::value;
+                    const int ri = q * kMaxChunk + c;
+                    const float4 A = recA[ri];
+                    bool act = A.x <= s.ap;
+                    const int slot = __float_as_int(A.w);
+                    if (hard_cut && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
+                        act = !exact_outside_aperture(Pg, c0 + slot, p, t, s_ox[q], s_oy[q]);
                     float T, f;
                     int i0;
+                    bool ok;
                     if constexpr (EXACT) {
-                        const double qs = fma(r64.x, s.B, t_.A);
-                        const double qr = fma(r64.y, s.B, t_.A);
-                        double T2;
-                        if (!t_.guard) {
-                            T2 = sqrt_newton(qs) + sqrt_newton(qr);
-                        } else {
-                            T2 = (qs > 0.0 ? sqrt_newton(qs) : 0.0) + (qr > 0.0 ? sqrt_newton(qr) : 0.0);
-                        }
+                        const double2 B = reinterpret_cast<const double2 *>(recA + RECS)[ri];
+                        const double T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
                         // s + 2^31 keeps s in the mantissa with 21 fraction bits
                         const double v = T2 + magic;
                         const unsigned vh = (unsigned)__double2hiint(v), vl = (unsigned)__double2loint(v);
                         const unsigned iu = __funnelshift_r(vl, vh, 21);
-                        if (iu >= ns_m1) continue;   // also rejects s < 0 and NaN
-                        i0 = (int)iu;
+                        ok = act && iu < ns_m1;   // also rejects s < 0 and NaN
+                        i0 = ok ? (int)iu : 0;
                         f = __uint_as_float(0x3F800000u | ((vl & 0x1FFFFFu) << 2)) - 1.0f;
-                        T = t_.guard ? (float)T2 : double_to_float_trunc(T2);
+                        T = double_to_float_trunc(fmax(T2, 1e-30));
                     } else {
-                        T = traveltime<TT>(P, t_, s, r0, r1, r2);
+                        const float4 B = reinterpret_cast<const float4 *>(recA + RECS)[ri];
+                        float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if constexpr (HAS_C) Cc = reinterpret_cast<const float4 *>(recA + 2 * RECS)[ri];
+                        T = traveltime<TT>(P, ts, s, B, Cc);
                         float sidx = fmaf(T, s_scale, s_offset);
-                        if (!(sidx >= sg_lo && sidx <= sg_hi)) {
-                            if (!(sidx >= sr_lo && sidx <= sr_hi)) continue;
-                            if (!exact_sample_ok<TT>(Pg, c0 + c, p, t_base + r * 32, s_ox[q], s_oy[q])) continue;
+                        const bool fast_ok = sidx >= sg_lo && sidx <= sg_hi;
+                        const bool band = act && !fast_ok && sidx >= sr_lo && sidx <= sr_hi;
+                        if constexpr (SLOW) {   // re-decide the guard band in FP64
+                            ok = band && exact_sample_ok<TT>(Pg, c0 + slot, p, t, s_ox[q], s_oy[q]);
                             sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
+                        } else {
+                            ok = act && fast_ok;
+                            pend |= band;
                         }
+                        sidx = ok ? sidx : 0.f;
                         const float fl = __fadd_rd(sidx, 8388608.f);
                         i0 = __float_as_int(fl) - 0x4B000000;
                         f = sidx - (fl - 8388608.f);
                     }
+                    const unsigned char *row = ampb + slot * row_bytes;
                     const float a0 = amp_at<AMP>(row, i0);
                     const float a1 = amp_at<AMP>(row, i0 + 1);
                     const float amp = fmaf(f, a1 - a0, a0);
-                    float w = r0.w;
-                    const float x = fmaf(r0.z, s.itw, s.tsn);
-                    if (x > 0.f) w *= 0.5f + 0.5f * __cosf(3.14159265358979f * x);
+                    float w = ok ? A.y : 0.f;
+                    if constexpr (TAPER) {
+                        const float x = fmaf(A.x, s.itw, s.tsn);
+                        w *= x > 0.f ? taper_weight(x) : 1.f;
+                    }
                     const float rT = rcp_approx(T);
-                    float gw = 1.f;
-                    if (nw) {
-                        gw = s.K * rT;
-                        if (nw == 2) gw *= rT;
+                    float gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
+                    gw = T > ts.tg ? gw : 1.f;   // the reference applies them only for T > 1 ms
+                    if (aa_on) {
+                        const float sth = fminf(A.z * s.ivw_t * rT, 1.f);
+                        const float aa = fmaxf(0.f, 1.f - fmaxf(s.aaA * sth, aa_cB));
+                        gw = (sth >= 0.01f && T >= ts.tguard) ? gw * aa : gw;
                     }
-                    constexpr bool kSmallT = (TT == TT_CURVED || TT == TT_CURVED_VTI);
-                    if ((kSmallT || t_.guard) && !(T > t_.tguard)) gw = 1.f;
-                    if constexpr (AA) {
-                        if (T >= t_.tguard) {
-                            const float sth = fminf(r1.x * s.ivw_t * rT, 1.f);
-                            if (sth >= 0.01f) gw *= fmaxf(0.f, 1.f - fmaxf(aa_cA * sth * s.ivw, aa_cB));
-                        }
+                    return amp * (w * gw);
+                };
+                using F = std::false_type;
+                using Tr = std::true_type;
+                float a = 0.f;
+#pragma unroll 4
+                for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{});
+#pragma unroll 2
+                for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{});
+                if constexpr (!EXACT) {
+                    if (__any_sync(0xffffffffu, pend)) {
+                        for (int c = 0; c < n; ++c) a += pair(c, Tr{}, Tr{});
                     }
-                    acc[g][r] = fmaf(amp, w * gw, acc[g][r]);
                 }
+                s_acc[(q * R + r) * kThreads + tid] += a;
             }
         }
-        // fold chunk partials into the compensated sums
-#pragma unroll
-        for (int g = 0; g < PBG; ++g)
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float y = acc[g][r];
-                if (P.compensated) {
-                    const float sum = hi[g][r] + y;
-                    const float bp = sum - hi[g][r];
-                    lo[g][r] += (hi[g][r] - (sum - bp)) + (y - bp);
-                    hi[g][r] = sum;
-                } else {
-                    hi[g][r] += y;
-                }
-                acc[g][r] = 0.f;
-            }
-        __syncthreads();   // buffer `buf` and the records are free again
-        if (P.bulk && tid == 0 && k + 2 < n_chunks) {
+
+        // ---------------- records of chunk k+1 (its copy was issued a chunk ago)
+        bool timeout = false;
+        if (k + 1 < n_chunks) {
+            const int nb = buf ^ 1;
+            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((k + 1) >> 1) & 1));
+            if (!timeout) build_records(k + 1, nb);
+        }
+        if ((k + 1) % flush_every == 0) flush();
+        if (__syncthreads_or(timeout)) {   // also: buffer `buf` is free again
+            aborted = true;
+            break;
+        }
+        if (tid == 0 && k + 2 < n_chunks) {
             fence_proxy_async();
             issue_chunk(k + 2, buf);
         }
     }
 
     if (aborted) {
-        // a copy never completed: report, drain what is still in flight, and leave
+        // a copy never completed: report, drain what may still be in flight, leave
         if (tid == 0) {
             atomicOr(P.err, (int)KERR_WAIT_TIMEOUT);
             mbar_wait(bar0, 0);
@@ -626,26 +678,19 @@ migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
         return;
     }
 
-    // ---------------- epilogue: image += sum; fold += count
+    // ---------------- epilogue: image += the last partials; fold += count
+    flush();
+    if (P.fold && P.fold3d) {
 #pragma unroll
-    for (int g = 0; g < PBG; ++g) {
-        const int q = wp * PBG + g;
-        const int p = s_pid[q];
-        if (p < 0) continue;
-        const int cnt = s_fold[q];
+        for (int q = 0; q < PB; ++q) {
+            const int p = s_pid[q];
+            if (p < 0) continue;
+            const int cnt = s_fold[q];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int t = t_base + r * 32;
-            if (t >= P.nt) continue;
-            const int64_t idx = (int64_t)p * P.nt + t;
-            if (P.image_f32) {
-                float *img = reinterpret_cast<float *>(P.image);
-                img[idx] += hi[g][r] + lo[g][r];
-            } else {
-                double *img = reinterpret_cast<double *>(P.image);
-                img[idx] += (double)hi[g][r] + (double)lo[g][r];
+            for (int r = 0; r < R; ++r) {
+                const int t = t_lane + r * kThreads;
+                if (t < P.nt) P.fold[(int64_t)p * P.nt + t] += cnt;
             }
-            if (P.fold && P.fold3d) P.fold[idx] += cnt;
         }
     }
     if (P.fold && !P.fold3d && blockIdx.y == 0 && tid < PB) {
@@ -654,9 +699,14 @@ migrate_staged_kernel(const KParams P, const KParams *__restrict__ Pg) {
     }
 }
 
-// Per-(pillar|0, time) tables: {1/v^2, aperture, 1/v, eta} and 1/(v dt)^2,
-// evaluated in FP64 as numba_cpu_optimized.py:378-399 does, the first rounded
-// once to FP32.
-__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab);
+// Per-time tables: 2 x float4 {t0h2, Kt, tg, tguard}, {vz, vz2, 1/vz, t0==0}
+// and double A, per output time; per-(pillar|0, time) tables {1/v^2,
+// aperture, 1/v, eta} and 1/(v dt)^2; all evaluated in FP64 as
+// numba_cpu_optimized.py:378-399 does, the float4s rounded once to FP32.
+__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
+                                double *ttimeA);
+
+// Packed FP64 trace geometry, kGeoDoubles per trace: sx sy rx ry mx my w 0.
+__global__ void pack_geometry(const KParams P, double *geo);
 
 }  // namespace pstm

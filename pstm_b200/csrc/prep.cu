@@ -3,10 +3,12 @@
 
 namespace pstm {
 
-// {1/v^2, aperture, 1/v, eta} and 1/(v dt)^2 per (pillar or 0, output time),
-// evaluated in FP64 as numba_cpu_optimized.py:378-399 does; the float4 is
-// rounded once to FP32.
-__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab) {
+// Per-(pillar or 0, output time): {1/v^2, aperture, 1/v, eta} and 1/(v dt)^2;
+// per output time: {t0h2, Kt, tg, tguard}, {vz, vz2, 1/vz, t0 == 0} and
+// (t0/(2 dt))^2.  Evaluated in FP64 as numba_cpu_optimized.py:378-399 does;
+// the float4s are rounded once to FP32.
+__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
+                                double *ttimeA) {
     const int64_t n = n_p * P.nt;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -21,6 +23,44 @@ __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, doubl
         if (P.eta) eta = P.eta3d ? P.eta[p * P.nt + t] : P.eta[t];
         tab[i] = make_float4((float)(1.0 / (v * v)), (float)ap, (float)(1.0 / v), (float)eta);
         btab[i] = 1.0 / (v * v * P.dt_s * P.dt_s);
+        if (p == 0) {
+            const double tu = P.exact_units ? P.dt_s : 1.0;
+            const double tguard = 0.001 / tu;
+            // straight rays and VTI have T >= t0, so only t0 < 1.1 ms can give T <= 1 ms;
+            // the curved-ray leg of the reference tends to 0 at large offsets
+            const bool small_t = P.curved_kind || t0 < 0.0011;
+            float vz = 0.f, vz2 = 0.f, ivwc = 0.f;
+            if (P.curved_kind) {
+                const double z = P.cr_k_zero ? P.cr_v0 * (t0 * 0.5)
+                                             : (P.cr_v0 / P.cr_k) * (exp(P.cr_k * (t0 * 0.5)) - 1.0);
+                const double vzd = P.cr_v0 + P.cr_k * z;
+                vz = (float)vzd;
+                vz2 = (float)(vzd * vzd);
+                ivwc = (float)(1.0 / vzd);
+            }
+            ttime[2 * t] = make_float4((float)((t0 * 0.5) * (t0 * 0.5)), P.obliquity ? (float)(t0 / tu) : 1.f,
+                                       small_t ? (float)tguard : -1.f, (float)tguard);
+            ttime[2 * t + 1] = make_float4(vz, vz2, ivwc, t0 > 0.0 ? 0.f : 1.f);
+            const double th = t0 * 0.5 / P.dt_s;
+            ttimeA[t] = fmax(th * th, 1e-300);
+        }
+    }
+}
+
+// Packed FP64 trace geometry for the bulk copies: kGeoDoubles per trace,
+// sx sy rx ry mx my w 0 (w = 1 when the caller gives no weights).
+__global__ void pack_geometry(const KParams P, double *geo) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n_traces;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double *g = geo + i * kGeoDoubles;
+        g[0] = P.sx[i];
+        g[1] = P.sy[i];
+        g[2] = P.rx[i];
+        g[3] = P.ry[i];
+        g[4] = P.mx[i];
+        g[5] = P.my[i];
+        g[6] = P.w ? P.w[i] : 1.0;
+        g[7] = 0.0;
     }
 }
 
