@@ -257,8 +257,8 @@ def main_ours(args):
     value = world * args.steps * pairs_per_step / (ms / 1e3)
     clocks = clk.summary()
 
-    # ---- roofline of the migration kernel (one launch per step; the per-step
-    # table kernel is ~1e-5 of the step)
+    # ---- roofline of the migration kernel (one launch per step; the table and
+    # geometry-packing kernels of a step take ~1e-4 of it)
     per_launch_s = ms / 1e3 / args.steps
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     mufu_peak = 148 * 16 * sm_mhz * 1e6          # MUFU ops/s, derived: 148 SMs x 16/clk x median SM clock
@@ -310,8 +310,8 @@ def main_ours(args):
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        for j in range(args.e2e_steps):
-            ke.migrate_tile(htb, *h_tiles[my_tiles[j % len(my_tiles)]])
+        for j in range(args.e2e_steps):   # the same tiles as the timed device steps
+            ke.migrate_tile(htb, *h_tiles[my_tiles[args.warmup + j % args.steps]])
         e2e_s = time.perf_counter() - t0
         if dist:
             t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -346,11 +346,12 @@ def main_ours(args):
                                    "3.2 km patch, 3-D v_rms, AA on, 5 km aperture; one step = "
                                    f"{T}x{T}x{NT} output tile (pillars x samples)",
                        "traces": N, "tile": [T, T, NT], "grid": [GRID, GRID, NT], "traveltime": "straight_ray",
-                       "trace_dtype": args.dtype, "precision": args.precision, "accumulate": "fp32 compensated -> f64 image",
+                       "trace_dtype": args.dtype, "precision": args.precision,
+                       "accumulate": "fp32 per trace chunk -> f64 image",
                        "l2": "inputs larger than L2 (trace panel > 126 MB), no flush",
                        "parallelism": f"replicas x{world} (disjoint tiles)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": 2 * args.steps, "clocks": clocks,
+            "gpu_launches": 3 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -131,7 +131,7 @@ struct TimeState {
     float tguard;          // 1 ms in the unit of T
     float vz, vz2, ivwc;   // curved: velocity at image depth, 1/vz
     bool tzero;
-    double A;              // EXACT: (t0 / (2 dt))^2 (at least 1e-300)
+    double A;              // EXACT: (t0 / (2 dt))^2 (at least 1e-20)
 };
 
 // Quantities that depend on (pillar, time).
@@ -341,7 +341,9 @@ __host__ __device__ constexpr int geo_buffer_bytes() { return kMaxChunk * kGeoDo
 __host__ __device__ constexpr int partial_bytes(int PB, int R) { return PB * R * kThreads * 4; }
 
 // ---------------------------------------------------------------- the kernel
-template <int TT, int AMP, bool VEL3D, bool EXACT>
+// W2: spreading and obliquity both on (the common case), else the weight
+// exponent is chosen at run time.
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
 __global__ void __launch_bounds__(kThreads, 1)
 migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
@@ -569,14 +571,15 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                 bool pend = false;   // FP32 path: some pair lies in a trace-end guard band
 
                 // contribution of record c (slot in the sorted order) to this lane's time
-                auto pair = [&](int c, auto taper_c, auto slow_c) -> float {
+                auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c) -> float {
                     constexpr bool TAPER = decltype(taper_c)::value;
                     constexpr bool SLOW = decltype(slow_c)::value;
+                    constexpr bool HARD = decltype(hard_c)::value;
                     const int ri = q * kMaxChunk + c;
                     const float4 A = recA[ri];
                     bool act = A.x <= s.ap;
                     const int slot = __float_as_int(A.w);
-                    if (hard_cut && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
+                    if (HARD && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
                         act = !exact_outside_aperture(Pg, c0 + slot, p, t, s_ox[q], s_oy[q]);
                     float T, f;
                     int i0;
@@ -591,7 +594,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                         ok = act && iu < ns_m1;   // also rejects s < 0 and NaN
                         i0 = ok ? (int)iu : 0;
                         f = __uint_as_float(0x3F800000u | ((vl & 0x1FFFFFu) << 2)) - 1.0f;
-                        T = double_to_float_trunc(fmax(T2, 1e-30));
+                        T = double_to_float_trunc(T2);   // T2 >= 2e-10: A >= 1e-20
                     } else {
                         const float4 B = reinterpret_cast<const float4 *>(recA + RECS)[ri];
                         float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -622,7 +625,9 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                         w *= x > 0.f ? taper_weight(x) : 1.f;
                     }
                     const float rT = rcp_approx(T);
-                    float gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
+                    float gw;
+                    if constexpr (W2) gw = s.K * rT * rT;
+                    else gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
                     gw = T > ts.tg ? gw : 1.f;   // the reference applies them only for T > 1 ms
                     if (aa_on) {
                         const float sth = fminf(A.z * s.ivw_t * rT, 1.f);
@@ -634,13 +639,18 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                 using F = std::false_type;
                 using Tr = std::true_type;
                 float a = 0.f;
+                if (!hard_cut) {
 #pragma unroll 4
-                for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{});
+                    for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{});
 #pragma unroll 2
-                for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{});
+                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{});
+                } else {   // no taper: the aperture edge is a hard cut, ties are decided in FP64
+#pragma unroll 2
+                    for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{});
+                }
                 if constexpr (!EXACT) {
                     if (__any_sync(0xffffffffu, pend)) {
-                        for (int c = 0; c < n; ++c) a += pair(c, Tr{}, Tr{});
+                        for (int c = 0; c < n; ++c) a += pair(c, Tr{}, Tr{}, Tr{});
                     }
                 }
                 s_acc[(q * R + r) * kThreads + tid] += a;

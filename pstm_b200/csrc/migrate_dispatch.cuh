@@ -6,9 +6,9 @@
 
 namespace pstm {
 
-template <int TT, int AMP, bool VEL3D, bool EXACT>
-static cudaError_t launch_one(const KParams &P, const KParams *Pg, dim3 grid, size_t smem, cudaStream_t st) {
-    auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT>;
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+static cudaError_t launch_w(const KParams &P, const KParams *Pg, dim3 grid, size_t smem, cudaStream_t st) {
+    auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
     static size_t configured = 0;   // dynamic shared memory opt-in, per instantiation
     if (smem > configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -17,6 +17,12 @@ static cudaError_t launch_one(const KParams &P, const KParams *Pg, dim3 grid, si
     }
     kern<<<grid, kThreads, smem, st>>>(P, Pg);
     return cudaGetLastError();
+}
+
+template <int TT, int AMP, bool VEL3D, bool EXACT>
+static cudaError_t launch_one(const KParams &P, const KParams *Pg, dim3 grid, size_t smem, cudaStream_t st) {
+    if (P.spreading && P.obliquity) return launch_w<TT, AMP, VEL3D, EXACT, true>(P, Pg, grid, smem, st);
+    return launch_w<TT, AMP, VEL3D, EXACT, false>(P, Pg, grid, smem, st);
 }
 
 template <int TT, bool EXACT>

@@ -42,7 +42,7 @@ __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, doubl
                                        small_t ? (float)tguard : -1.f, (float)tguard);
             ttime[2 * t + 1] = make_float4(vz, vz2, ivwc, t0 > 0.0 ? 0.f : 1.f);
             const double th = t0 * 0.5 / P.dt_s;
-            ttimeA[t] = fmax(th * th, 1e-300);
+            ttimeA[t] = fmax(th * th, 1e-20);   // keeps the FP64 legs > 0 at t0 = 0
         }
     }
 }
