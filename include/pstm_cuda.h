@@ -149,12 +149,34 @@ int32_t pstm_cuda_migrate_tile_host(void *ctx, const pstm_traces_desc *traces,
                                     const pstm_velocity_desc *velocity,
                                     const pstm_params *params);
 
+/* Allocation-free variant of pstm_cuda_migrate_tile_dev; it has no
+ * counterpart in the reference.  It is for callers that cannot allocate
+ * device memory while they run -- an application whose memory manager owns
+ * the whole GPU, or a job that must not stall the device (cudaMalloc
+ * synchronises it) or fail on an allocation after start-up.  It needs no
+ * context and allocates nothing: its scratch (tables, packed geometry, launch
+ * parameters) is a fixed 16 MiB array in this library's device memory, held
+ * by every device that loads the library until the process exits.  Limits of
+ * one call: n_traces <= 131072, nt <= 8192, and (nx*ny if the velocity or eta
+ * is 3-D, else 1) * nt <= 262144; larger inputs are rejected with
+ * PSTM_ERR_INVALID_ARGUMENT (split the traces over several calls: image and
+ * fold accumulate).  Inputs and outputs are device pointers; work is queued
+ * on `stream` (NULL = the legacy default stream) of the calling thread's
+ * current device.  The first call on a device looks up the array's address;
+ * make that first call before any stream capture.  All calls share the array,
+ * so calls that overlap on the GPU race: serialise them.  Errors are reported
+ * by pstm_cuda_last_error(NULL). */
+int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                       const pstm_velocity_desc *velocity, const pstm_params *params,
+                                       void *stream);
+
 /* Wait for all work queued on the context's stream.  Replaces
  * MigrationKernel.synchronize, pstm/kernels/base.py:315. */
 int32_t pstm_cuda_synchronize(void *ctx);
 
-/* Message of the last failing call on this context (or of the last failing
- * pstm_cuda_create when ctx is NULL).  Reference: the RuntimeError text the
+/* Message of the last failing call on this context (or, when ctx is NULL, of
+ * the calling thread's last failing pstm_cuda_create or
+ * pstm_cuda_migrate_tile_noalloc).  Reference: the RuntimeError text the
  * Metal backend raises, metal_compiled.py:763-764. */
 const char *pstm_cuda_last_error(void *ctx);
 

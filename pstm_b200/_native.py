@@ -77,6 +77,8 @@ SIGNATURES = {
                                                     ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
     "pstm_cuda_migrate_tile_host": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                      ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
+    "pstm_cuda_migrate_tile_noalloc": (ctypes.c_int32, [ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
+                                                        ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
 }

@@ -11,6 +11,7 @@
 #include "pstm_cuda.h"
 #include "kparams.h"
 #include "migrate_dispatch.cuh"
+#include "plan.h"
 
 namespace pstm {
 template <int TT>
@@ -21,6 +22,15 @@ __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, doubl
 }  // namespace pstm
 
 using namespace pstm;
+
+namespace {
+thread_local std::string g_create_err;
+}
+
+namespace pstm {
+// Message of the last failing call that has no context (create, noalloc).
+void set_context_free_error(const std::string &msg) { g_create_err = msg; }
+}  // namespace pstm
 
 namespace {
 
@@ -40,8 +50,6 @@ struct Ctx {
     int force_pb = 0;     // PSTM_CUDA_PB override of the pillars per CTA
     int smem_optin = 0;   // max dynamic shared memory per block
 };
-
-thread_local std::string g_create_err;
 
 int32_t fail(Ctx *c, int32_t code, const std::string &msg) {
     if (c) c->err = msg;
@@ -79,123 +87,14 @@ void release(DevBuf &b) {
     b.bytes = 0;
 }
 
-size_t amp_elem_bytes(int32_t dt) { return dt == PSTM_AMP_F32 ? 4 : 2; }
-
-// Largest double B such that the correctly rounded sqrt(B) <= a, i.e. the
-// FP64 predicate "sqrt(d2) > a" used by the reference equals "d2 > B".
-double sqrt_threshold(double a) {
-    double b = a * a;
-    while (std::sqrt(b) > a) b = std::nextafter(b, 0.0);
-    while (std::sqrt(std::nextafter(b, INFINITY)) <= a) b = std::nextafter(b, INFINITY);
-    return b;
-}
+using plan::amp_elem_bytes;
+using plan::make_params;
 
 int32_t validate(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
                  const pstm_velocity_desc *vel, const pstm_params *prm) {
-    if (!tr || !out || !vel || !prm) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null descriptor");
-    if (tr->n_traces < 0) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "n_traces < 0");
-    if (tr->n_samples < 2) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "n_samples must be >= 2");
-    if (tr->amp_dtype < PSTM_AMP_F32 || tr->amp_dtype > PSTM_AMP_F16)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown amplitude dtype");
-    if (tr->amp_row_stride < tr->n_samples)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "amp_row_stride < n_samples");
-    if (tr->n_traces > 0 && (!tr->amplitudes || !tr->source_x || !tr->source_y || !tr->receiver_x ||
-                             !tr->receiver_y || !tr->midpoint_x || !tr->midpoint_y))
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null trace array");
-    if (!(tr->sample_rate_ms > 0.0)) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "sample_rate_ms must be > 0");
-    if (out->nx <= 0 || out->ny <= 0 || out->nt <= 0)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "empty output tile");
-    if (!out->image) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null image");
-    if (out->image_dtype != PSTM_IMAGE_F64 && out->image_dtype != PSTM_IMAGE_F32)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown image dtype");
-    if (!out->t_axis_ms) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null t axis");
-    if ((!out->x_grid || !out->y_grid) && (!out->x_axis || !out->y_axis))
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "need x/y axes or x/y grids");
-    if ((out->x_grid == nullptr) != (out->y_grid == nullptr))
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "x_grid and y_grid must be given together");
-    if (!vel->vrms) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null velocity");
-    if (prm->traveltime < PSTM_TT_STRAIGHT || prm->traveltime > PSTM_TT_CURVED_VTI)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown traveltime kind");
-    if (prm->precision != PSTM_PREC_EXACT && prm->precision != PSTM_PREC_FAST)
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "unknown precision");
-    if (!(prm->max_aperture_m >= 0.0) || !(prm->taper_fraction >= 0.0) || !(prm->taper_fraction <= 1.0))
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "bad aperture/taper parameters");
-    if ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) && !(prm->curved_v0 > 0.0))
-        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "curved_v0 must be > 0");
-    return PSTM_OK;
-}
-
-KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
-                    const pstm_params *prm, int PB) {
-    KParams P;
-    std::memset(&P, 0, sizeof(P));
-    P.amps = tr->amplitudes;
-    P.amp_stride = tr->amp_row_stride;
-    P.n_traces = tr->n_traces;
-    P.ns = tr->n_samples;
-    P.elem = (int32_t)amp_elem_bytes(tr->amp_dtype);
-    P.sx = tr->source_x; P.sy = tr->source_y;
-    P.rx = tr->receiver_x; P.ry = tr->receiver_y;
-    P.mx = tr->midpoint_x; P.my = tr->midpoint_y;
-    P.w = tr->weights;
-    P.dt_s = tr->sample_rate_ms / 1000.0;
-    P.tstart_s = tr->start_time_ms / 1000.0;
-    P.s_scale = (float)(1.0 / P.dt_s);
-    P.s_offset = (float)(-P.tstart_s / P.dt_s);
-    const float g = 1e-2f;   // guard band in samples around the FP64 decision boundaries
-    const float smax = (float)(tr->n_samples - 1);
-    P.s_guard_lo = g;
-    P.s_guard_hi = smax - g;
-    P.s_rej_lo = -g;
-    P.s_rej_hi = smax + g;
-    P.s_max_clamp = std::nextafter(smax, 0.0f);
-    P.s_magic = 2147483648.0 - P.tstart_s / P.dt_s;
-    P.inv_dt_f = (float)(1.0 / P.dt_s);
-
-    P.image = out->image;
-    P.fold = out->fold;
-    P.image_f32 = out->image_dtype == PSTM_IMAGE_F32;
-    P.fold3d = out->fold_is_3d;
-    P.nx = out->nx; P.ny = out->ny; P.nt = out->nt;
-    P.xa = out->x_axis; P.ya = out->y_axis;
-    P.xg = out->x_grid; P.yg = out->y_grid;
-    P.ta = out->t_axis_ms;
-
-    P.vrms = vel->vrms;
-    P.vel3d = vel->is_3d;
-    P.eta = prm->eta;
-    P.eta3d = prm->eta ? prm->eta_is_3d : 0;
-    P.eta_const = prm->eta_constant;
-
-    P.max_ap = prm->max_aperture_m;
-    P.min_ap = prm->min_aperture_m;
-    P.tan_dip = std::tan(prm->max_dip_degrees * M_PI / 180.0);
-    P.taper = prm->taper_fraction;
-    P.fold_d2_max = sqrt_threshold(prm->max_aperture_m);
-    P.ap_max_f = (float)prm->max_aperture_m;
-    P.taper_f = (float)prm->taper_fraction;
-    P.spreading = prm->apply_spreading ? 1 : 0;
-    P.obliquity = prm->apply_obliquity ? 1 : 0;
-    P.aa = prm->aa_enabled ? 1 : 0;
-    const double gmax = prm->grid_dx > prm->grid_dy ? prm->grid_dx : prm->grid_dy;
-    P.aa_cA = (float)(4.0 * gmax * prm->aa_dominant_freq);
-    P.aa_cB = (float)(prm->aa_dominant_freq / 500.0);
-    P.cr_v0 = prm->curved_v0;
-    P.cr_k = prm->curved_k;
-    P.cr_v0f = (float)prm->curved_v0;
-    P.cr_kf = (float)prm->curved_k;
-    P.cr_k_zero = std::fabs(prm->curved_k) < 1e-10 ? 1 : 0;
-    P.cr_inv_k_ln2 = P.cr_k_zero ? 0.f : (float)(M_LN2 / prm->curved_k);
-    P.compensated = prm->compensated ? 1 : 0;
-
-    // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)
-    int py = PB, px = 1;
-    while (py > 1 && py > out->ny) { py /= 2; px *= 2; }
-    if (py == PB && PB >= 4) { py = PB / 2; px = 2; }
-    P.px = px;
-    P.py = py;
-    P.n_pblk_y = (out->ny + py - 1) / py;
-    return P;
+    const char *msg = "";
+    const int32_t rc = plan::check_args(tr, out, vel, prm, msg);
+    return rc ? fail(c, rc, msg) : PSTM_OK;
 }
 
 int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
@@ -205,12 +104,8 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     if (injected("migrate")) return fail(c, PSTM_ERR_INJECTED, "injected fault: migrate");
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
-    // output times per lane: the whole output trace in one CTA where it fits
-    int R = (out->nt + kThreads - 1) / kThreads;
-    if (R > 8) R = 8;
-    if (c->force_r >= 1 && c->force_r <= 8) R = c->force_r;
-    int PB = R <= 1 ? 8 : 4;
-    if (c->force_pb >= 1 && c->force_pb <= kMaxPB) PB = c->force_pb;
+    int R, PB;
+    plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB);
     KParams P = make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // nothing to add: image += 0, fold += 0
 
@@ -258,25 +153,9 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     // shared-memory staging of trace rows: pitch rounded up to 16 bytes; TMA
     // bulk copies when the rows are 16-byte aligned and the padded row is
     // inside the caller's stride, else a plain cooperative copy
-    const int eb = P.elem;
-    const int per16 = 16 / eb;
-    const int pitch = (tr->n_samples + per16 - 1) / per16 * per16;
-    const bool aligned = ((uintptr_t)tr->amplitudes % 16 == 0) && ((tr->amp_row_stride * eb) % 16 == 0);
-    P.pitch = pitch;
-    P.bulk = (aligned && tr->amp_row_stride >= pitch) ? 1 : 0;
-    const bool has_c = prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI;
-    const size_t fixed = 2 * (size_t)geo_buffer_bytes() + 2 * (size_t)record_buffer_bytes(PB, has_c) +
-                         (size_t)partial_bytes(PB, R);
-    const size_t static_bytes = 3072;   // s_ox/s_oy/s_pid/s_fold/s_rank/barriers, rounded up
-    const size_t budget = (size_t)c->smem_optin > fixed + static_bytes ? c->smem_optin - fixed - static_bytes : 0;
-    int chunk = (int)(budget / (2 * (size_t)pitch * eb));
-    if (chunk > kMaxChunk) chunk = kMaxChunk;
-    if (chunk < 1) return fail(c, PSTM_ERR_UNSUPPORTED, "trace rows too long to stage in shared memory");
-    P.chunk = chunk;
-    P.pb = PB;
-    P.r_per_lane = R;
-    P.flush_every = 16;
-    const size_t smem = 2 * (size_t)chunk * pitch * eb + fixed;
+    size_t smem = 0;
+    if (!plan::plan_staging(P, tr, prm, PB, R, c->smem_optin, smem))
+        return fail(c, PSTM_ERR_UNSUPPORTED, "trace rows too long to stage in shared memory");
 
     // a device copy of the launch parameters for the kernel's rare FP64 paths
     e = ensure(c->kparams, sizeof(KParams));
