@@ -45,6 +45,11 @@ UNIT = "pairs/s"
 FLOP_PER_PAIR = 20
 MUFU_PER_PAIR = 4
 
+# DRAM traffic of one 64 x 64 x 1500 tile launch per trace of the panel, from an
+# ncu capture (dram__bytes) of the same launch at 32,768 traces: 14.45 GB; the
+# traffic grows in proportion to the traces streamed (profiles/migrate_kernel_case2.md)
+DRAM_BYTES_PER_TRACE_TILE64 = 14.45e9 / 32768
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -59,6 +64,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision-form measurement")
     return ap.parse_args()
 
 
@@ -67,8 +73,8 @@ GRID, NT, NS, DT_MS, DX = 256, 1500, 1500, 2.0, 12.5
 
 
 def tiles_of(tile):
-    n = GRID // tile
-    return [(i * tile, (i + 1) * tile, j * tile, (j + 1) * tile) for i in range(n) for j in range(n)]
+    from pstm_b200 import replicas
+    return replicas.grid_tiles(GRID, GRID, tile)
 
 
 def config():
@@ -185,6 +191,67 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ forms
+def accuracy_vs_fp64(kernel_factory, sv, cfg, n_tr, amps_host, pillars=2):
+    """Relative L2 of a form against the FP64 oracle on a pillars x pillars x nt
+    sample of the first tile against the first n_tr traces (host arrays)."""
+    from oracle import oracle
+    from pstm_b200.base import create_trace_block
+    out, vel = sv.tile(20, 20 + pillars, 20, 20 + pillars)
+    tb = create_trace_block(amps_host[:n_tr], sv.s[:n_tr, 0], sv.s[:n_tr, 1], sv.r[:n_tr, 0], sv.r[:n_tr, 1],
+                            sample_rate_ms=DT_MS)
+    ref_out, _ = sv.tile(20, 20 + pillars, 20, 20 + pillars)
+    oracle.migrate(tb, ref_out, vel, cfg)
+    k = kernel_factory()
+    k.initialize(cfg)
+    k.migrate_tile(tb, out, vel)
+    k.cleanup()
+    return float(np.linalg.norm(out.image - ref_out.image) / np.linalg.norm(ref_out.image))
+
+
+def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg):
+    """Plain form (exact sample index, FP32 traces) and the precision form (BF16
+    traces, FP32 traveltime): pairs/s on the timed tiles and rel-L2 vs FP64."""
+    import dataclasses
+    import torch
+    from oracle import oracle
+    from pstm_b200 import replicas
+    from pstm_b200.cuda_kernel import CudaKernel
+    oracle.build()
+    n_acc = 1 << 16
+    amps_host = amps[:n_acc].float().cpu().numpy()
+    res = {}
+    specs = [("plain_exact_f32", "f32", "exact"), ("precision_bf16_fast", "bf16", "fast")]
+    for name, dt, prec in specs:
+        tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[dt]
+        tbf = tb if (dt == args.dtype and tdt == amps.dtype) else dataclasses.replace(tb, amplitudes=amps.to(tdt))
+        kf = CudaKernel(precision=prec)
+        kf.initialize(cfg)
+        kf.migrate_tile(tbf, *tile_args[my_tiles[0]])
+        torch.cuda.synchronize()
+        steps = min(2, args.steps)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for j in range(args.warmup, args.warmup + steps):
+            kf.migrate_tile(tbf, *tile_args[my_tiles[j]])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda")
+        kf.cleanup()
+        host = amps_host if dt == "f32" else amps[:n_acc].to(tdt).float().cpu().numpy()
+        err = accuracy_vs_fp64(lambda: CudaKernel(precision=prec, trace_dtype=dt), sv, cfg, n_acc, host)
+        if dt != "f32":   # the FP64 reference of a 16-bit form is fed the FP32 traces
+            err_vs_f32 = accuracy_vs_fp64(lambda: CudaKernel(precision=prec, trace_dtype=dt), sv, cfg, n_acc,
+                                          amps_host)
+        else:
+            err_vs_f32 = err
+        res[name] = {"value": world * steps * pairs_per_step / (ms / 1e3), "unit": UNIT,
+                     "trace_dtype": dt, "traveltime": prec, "steps": steps,
+                     "rel_l2_vs_fp64": err_vs_f32,
+                     "rel_l2_sample": f"2x2 pillars x {NT} samples x {n_acc} traces, FP64 oracle on FP32 traces"}
+    return res
+
+
 # ------------------------------------------------------------------ our arm
 def main_ours(args):
     import torch
@@ -213,8 +280,9 @@ def main_ours(args):
     offset = dev(np.hypot(sv.r[:, 0] - sv.s[:, 0], sv.r[:, 1] - sv.s[:, 1]))
     tb = TraceBlock(amplitudes=amps, offset=offset, sample_rate_ms=DT_MS, start_time_ms=0.0, **geo)
     cfg = config()
+    from pstm_b200 import replicas
     tiles = tiles_of(args.tile)
-    my_tiles = [tiles[(rank + j * world) % len(tiles)] for j in range(args.warmup + args.steps)]
+    my_tiles = replicas.rank_schedule(tiles, rank, world, args.warmup + args.steps)
     T = args.tile
     img = torch.zeros((T, T, NT), dtype=torch.float64, device="cuda")
     fold = torch.zeros((T, T, NT), dtype=torch.int32, device="cuda")
@@ -249,11 +317,7 @@ def main_ours(args):
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda")
     value = world * args.steps * pairs_per_step / (ms / 1e3)
     clocks = clk.summary()
 
@@ -280,7 +344,8 @@ def main_ours(args):
                  "peak_tflops": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12},
         "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
                 "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes},
-        "traffic": None,
+        "traffic": (DRAM_BYTES_PER_TRACE_TILE64 * N / 1e9) if T == 64 else None,
+        "traffic_unit": "GB per launch (ncu dram__bytes at 32,768 traces, scaled by traces)",
     }
 
     # ---- end to end through the public API with pinned host buffers
@@ -312,11 +377,7 @@ def main_ours(args):
         t0 = time.perf_counter()
         for j in range(args.e2e_steps):   # the same tiles as the timed device steps
             ke.migrate_tile(htb, *h_tiles[my_tiles[args.warmup + j % args.steps]])
-        e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist, device="cuda")
         h2d = amps_np.nbytes + sum(htb.__dict__[kk].nbytes for kk in geo) + T * T * NT * (8 + 8 + 4) + \
             3 * T * 8 + NT * 8
         d2h = T * T * NT * (8 + 4)
@@ -324,6 +385,10 @@ def main_ours(args):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "steps": args.e2e_steps, "timer": "perf_counter around synchronous migrate_tile calls"}
         ke.cleanup()
+
+    forms = None
+    if not args.no_forms:
+        forms = measure_forms(args, k, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -350,7 +415,7 @@ def main_ours(args):
                        "accumulate": "fp32 per trace chunk -> f64 image",
                        "l2": "inputs larger than L2 (trace panel > 126 MB), no flush",
                        "parallelism": f"replicas x{world} (disjoint tiles)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "forms": forms,
             "gpu_launches": 3 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
