@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define PSTM_CUDA_ABI_VERSION 1
+#define PSTM_CUDA_ABI_VERSION 2
 
 typedef enum {
     PSTM_OK = 0,
@@ -169,6 +169,58 @@ int32_t pstm_cuda_migrate_tile_host(void *ctx, const pstm_traces_desc *traces,
 int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *traces, const pstm_output_desc *output,
                                        const pstm_velocity_desc *velocity, const pstm_params *params,
                                        void *stream);
+
+/* One output of the batched form: a contiguous range of the batch's traces and
+ * its own image and fold.  Reference: one bin of the gather-bin loop,
+ * pstm/pipeline/executor.py:960-975, which migrates every offset/OVT bin into
+ * its own volume (_migrate_single_bin, executor.py:977). */
+typedef struct {
+    int64_t trace_begin;          /* first trace of the bin in the traces descriptor */
+    int64_t n_traces;             /* traces of the bin, contiguous */
+    void *image;                  /* device, (nx, ny, nt) of output->image_dtype, += */
+    int32_t *fold;                /* device, nullable; shaped as output->fold_is_3d says */
+} pstm_bin_desc;
+
+/* Launch shape chosen by pstm_cuda_autotune_bins. */
+typedef struct {
+    int32_t pillars_per_cta;      /* output traces one CTA migrates together */
+    int32_t times_per_lane;       /* output times per thread (512 * this per CTA) */
+    int32_t traces_per_chunk;     /* depth of the staged trace panel */
+    int32_t n_candidates;         /* shapes timed */
+    float best_ms;                /* time of the chosen shape on the tuning sample */
+    float default_ms;             /* time of the untuned default shape on the same sample */
+} pstm_tune_result;
+
+/* Migrate many bins that share one output tile geometry, velocity and
+ * parameters in ONE persistent launch: one CTA per SM takes (bin, pillar
+ * block, time block) items from a work counter, the bins with the most traces
+ * first, so bins of very different sizes keep every SM busy.  The whole
+ * sequence (table preparation, geometry packing, the launch) is captured in a
+ * CUDA graph that the context keeps and replays while the arguments repeat;
+ * new arguments re-capture it.  `output` gives the tile geometry (its image
+ * and fold pointers are ignored; each bin has its own, and they must not
+ * overlap).  Device pointers; asynchronous on `stream` as
+ * pstm_cuda_migrate_tile_dev; at most 4096 bins.  Uses the shape that
+ * pstm_cuda_autotune_bins chose for this class of workload, if it ran.
+ * Replaces the per-bin sequence of migrate_tile calls of the executor
+ * (executor.py:960-975 -> :1730). */
+int32_t pstm_cuda_migrate_bins_dev(void *ctx, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                   const pstm_velocity_desc *velocity, const pstm_params *params,
+                                   const pstm_bin_desc *bins, int32_t n_bins, void *stream);
+
+/* Autotuner of the batched form (no reference counterpart; the reference
+ * picks its threadgroup shape by a fixed rule, compute_optimal_threadgroup,
+ * pstm/kernels/metal_compiled.py:292-335, used at :742-743).  Times
+ * candidate launch shapes (pillars per CTA, output times per lane, traces per
+ * chunk) on a sample of the batch -- the largest bins, clipped so that one
+ * candidate migrates about `pairs_per_candidate` sample-trace pairs (0: 2^36)
+ * into scratch outputs of the context -- keeps the fastest for this class of
+ * workload (traveltime kind, trace dtype, 3-D velocity, precision, nt, ns) and
+ * reports it.  Synchronous; the bins' images and folds are not touched. */
+int32_t pstm_cuda_autotune_bins(void *ctx, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                const pstm_velocity_desc *velocity, const pstm_params *params,
+                                const pstm_bin_desc *bins, int32_t n_bins, int64_t pairs_per_candidate,
+                                pstm_tune_result *result);
 
 /* Wait for all work queued on the context's stream.  Replaces
  * MigrationKernel.synchronize, pstm/kernels/base.py:315. */

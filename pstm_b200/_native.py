@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpstm_cuda.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # pstm_status
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_INITIALIZED, \
@@ -68,6 +68,18 @@ class Params(ctypes.Structure):
     ]
 
 
+class BinDesc(ctypes.Structure):
+    _fields_ = [("trace_begin", ctypes.c_int64), ("n_traces", ctypes.c_int64), ("image", _vp), ("fold", _vp)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("pillars_per_cta", ctypes.c_int32), ("times_per_lane", ctypes.c_int32),
+        ("traces_per_chunk", ctypes.c_int32), ("n_candidates", ctypes.c_int32),
+        ("best_ms", ctypes.c_float), ("default_ms", ctypes.c_float),
+    ]
+
+
 # name -> (restype, argtypes); the exported surface of include/pstm_cuda.h
 SIGNATURES = {
     "pstm_cuda_abi_version": (ctypes.c_int32, []),
@@ -79,6 +91,13 @@ SIGNATURES = {
                                                      ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
     "pstm_cuda_migrate_tile_noalloc": (ctypes.c_int32, [ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                         ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
+    "pstm_cuda_migrate_bins_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
+                                                    ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params),
+                                                    ctypes.POINTER(BinDesc), ctypes.c_int32, _vp]),
+    "pstm_cuda_autotune_bins": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
+                                                 ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params),
+                                                 ctypes.POINTER(BinDesc), ctypes.c_int32, ctypes.c_int64,
+                                                 ctypes.POINTER(TuneResult)]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
 }

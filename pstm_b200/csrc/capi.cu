@@ -10,16 +10,9 @@
 
 #include "pstm_cuda.h"
 #include "kparams.h"
-#include "migrate_dispatch.cuh"
+#include "launch.h"
 #include "plan.h"
-
-namespace pstm {
-template <int TT>
-cudaError_t launch_migrate(const KParams &, const KParams *, int, bool, bool, dim3, size_t, cudaStream_t);
-__global__ void pack_geometry(const KParams P, double *geo);
-__global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
-                                double *ttimeA);
-}  // namespace pstm
+#include "ctx.h"
 
 using namespace pstm;
 
@@ -30,26 +23,8 @@ thread_local std::string g_create_err;
 namespace pstm {
 // Message of the last failing call that has no context (create, noalloc).
 void set_context_free_error(const std::string &msg) { g_create_err = msg; }
-}  // namespace pstm
 
-namespace {
-
-struct DevBuf {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-};
-
-struct Ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    DevBuf ttab, btab, ttime, ttimeA, kparams, errword, packed_geo;
-    // staging for the host-pointer path
-    DevBuf amps, geo[7], xa, ya, xg, yg, ta, vel, eta, image, fold;
-    int force_r = 0;      // PSTM_CUDA_R override of the output times per lane
-    int force_pb = 0;     // PSTM_CUDA_PB override of the pillars per CTA
-    int smem_optin = 0;   // max dynamic shared memory per block
-};
+namespace ctx {
 
 int32_t fail(Ctx *c, int32_t code, const std::string &msg) {
     if (c) c->err = msg;
@@ -86,6 +61,13 @@ void release(DevBuf &b) {
     b.ptr = nullptr;
     b.bytes = 0;
 }
+
+}  // namespace ctx
+}  // namespace pstm
+
+namespace {
+
+using namespace pstm::ctx;
 
 using plan::amp_elem_bytes;
 using plan::make_params;
@@ -169,14 +151,11 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     const int tb = kThreads * R;
     const int nblk_t = (out->nt + tb - 1) / tb;
     if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(c, PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
-    dim3 grid((unsigned)nblk_p, (unsigned)nblk_t);
-    const int amp = tr->amp_dtype;
-    switch (prm->traveltime) {
-    case PSTM_TT_STRAIGHT: e = launch_migrate<TT_STRAIGHT>(P, Pg, amp, per_pillar, exact, grid, smem, st); break;
-    case PSTM_TT_CURVED: e = launch_migrate<TT_CURVED>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    case PSTM_TT_VTI: e = launch_migrate<TT_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    default: e = launch_migrate<TT_CURVED_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    }
+    Launch L;
+    L.grid = dim3((unsigned)nblk_p, (unsigned)nblk_t);
+    L.smem = smem;
+    L.stream = st;
+    e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, exact, L);
     if (e != cudaSuccess) return cuda_fail(c, e, "migrate kernel launch");
     return PSTM_OK;
 }
@@ -258,6 +237,7 @@ void pstm_cuda_destroy(void *ctx) {
     for (auto &g : c->geo) release(g);
     release(c->xa); release(c->ya); release(c->xg); release(c->yg); release(c->ta);
     release(c->vel); release(c->eta); release(c->image); release(c->fold);
+    release_batch(c);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

@@ -12,6 +12,14 @@ enum TTKind { TT_STRAIGHT = 0, TT_CURVED = 1, TT_VTI = 2, TT_CURVED_VTI = 3 };
 // error bits a kernel can raise in *err
 enum KernelError { KERR_WAIT_TIMEOUT = 1 };
 
+// One output of the persistent form: its traces and its image/fold.
+struct BinWork {
+    int64_t trace0;              // first trace in the concatenated panel
+    int64_t n_traces;
+    void *image;
+    int32_t *fold;
+};
+
 struct KParams {
     // ---- traces ----
     const void *amps;
@@ -31,6 +39,7 @@ struct KParams {
 
     // ---- staging of trace rows in shared memory ----
     int32_t chunk;               // traces per chunk (<= kMaxChunk)
+    int32_t n_tblk;              // time blocks per output (persistent form)
     int32_t pb;                  // pillars per CTA (<= kMaxPB)
     int32_t r_per_lane;          // output times per lane (R)
     int32_t pitch;               // staged row pitch, elements (multiple of 16 bytes)

@@ -341,20 +341,42 @@ __host__ __device__ constexpr int geo_buffer_bytes() { return kMaxChunk * kGeoDo
 __host__ __device__ constexpr int partial_bytes(int PB, int R) { return PB * R * kThreads * 4; }
 
 // ---------------------------------------------------------------- the kernel
+// What one work item migrates: PB pillars x one block of 512*R output times of
+// one output image, against one contiguous range of traces.
+struct Item {
+    const unsigned char *amps;   // first amplitude row of the range
+    const double *geo;           // first packed trace of the range
+    int64_t trace0;              // global index of the first trace (FP64 re-decisions)
+    int64_t n_traces;
+    void *image;
+    int32_t *fold;
+    int pbx, pby, tblock;
+};
+
+// Shared-memory state of a CTA besides the dynamic buffers.
+struct CtaShared {
+    double ox[kMaxPB], oy[kMaxPB];
+    int pid[kMaxPB];
+    int fold[kMaxPB];
+    int rank[kMaxPB][kMaxChunk];
+    unsigned long long bar[2];
+    long long item;
+};
+
+// Migrates one item.  `chunk_base` counts the chunks this CTA staged before
+// (it selects the buffer and the mbarrier phase of every chunk).  Returns
+// false when a bounded wait gave up.
 // W2: spreading and obliquity both on (the common case), else the weight
 // exponent is chosen at run time.
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
-__global__ void __launch_bounds__(kThreads, 1)
-migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
-    static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
-    static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
+__device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__restrict__ Pg, const Item &it,
+                                             unsigned char *smem, CtaShared &sh, int64_t &chunk_base) {
     constexpr bool HAS_C = RecLayout<TT>::kHasC;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ double s_ox[kMaxPB], s_oy[kMaxPB];
-    __shared__ int s_pid[kMaxPB];
-    __shared__ int s_fold[kMaxPB];
-    __shared__ int s_rank[kMaxPB][kMaxChunk];
-    __shared__ __align__(8) unsigned long long s_bar[2];
+    double *const s_ox = sh.ox;
+    double *const s_oy = sh.oy;
+    int *const s_pid = sh.pid;
+    int *const s_fold = sh.fold;
+    auto &s_rank = sh.rank;
 
     const int PB = P.pb, R = P.r_per_lane;
     const int RECS = PB * kMaxChunk;
@@ -368,7 +390,8 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     float *const s_acc = reinterpret_cast<float *>(rec_base + 2 * REC_BYTES);   // [PB][R][kThreads]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int pbx = blockIdx.x / P.n_pblk_y, pby = blockIdx.x - pbx * P.n_pblk_y;
+    const int pbx = it.pbx, pby = it.pby;
+    __syncthreads();   // the previous item is done with the shared state
     if (tid < PB) {
         const int ix = pbx * P.px + tid / P.py, iy = pby * P.py + tid % P.py;
         const bool ok = (tid < P.px * P.py) && ix < P.nx && iy < P.ny;
@@ -378,13 +401,8 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
         s_ox[tid] = ok ? (P.xg ? P.xg[p] : P.xa[ix]) : 0.0;
         s_oy[tid] = ok ? (P.yg ? P.yg[p] : P.ya[iy]) : 0.0;
     }
-    const uint32_t bar0 = smem_u32(&s_bar[0]), bar1 = smem_u32(&s_bar[1]);
-    if (tid == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar1, 1);
-        fence_barrier_init();
-    }
-    const int t_lane = blockIdx.y * (kThreads * R) + tid;
+    const uint32_t bar0 = smem_u32(&sh.bar[0]), bar1 = smem_u32(&sh.bar[1]);
+    const int t_lane = it.tblock * (kThreads * R) + tid;
 
     // hot-loop constants in registers
     const float s_scale = P.s_scale, s_offset = P.s_offset;
@@ -397,7 +415,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     const bool aa_on = P.aa != 0;
     const bool hard_cut = !(P.taper_f > 0.f);
     const float one_m_taper = 1.f - P.taper_f;
-    const int64_t n_chunks = (P.n_traces + C - 1) / C;
+    const int64_t n_chunks = (it.n_traces + C - 1) / C;
     const int flush_every = P.flush_every;
 
     for (int i = tid; i < PB * R * kThreads; i += kThreads) s_acc[i] = 0.f;
@@ -406,13 +424,13 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     // rows when they are 16-byte aligned) into buffer b
     auto issue_chunk = [&](int64_t k, int b) {
         const int64_t c0 = k * C;
-        const int rows = (int)min((int64_t)C, P.n_traces - c0);
+        const int rows = (int)min((int64_t)C, it.n_traces - c0);
         const uint32_t bar = b ? bar1 : bar0;
         const uint32_t geo_bytes = (uint32_t)(rows * kGeoDoubles * 8);
         mbar_expect_tx(bar, geo_bytes + (P.bulk ? (uint32_t)(rows * row_bytes) : 0u));
-        bulk_g2s(smem_u32(geo_base + b * geo_buffer_bytes()), P.geo + c0 * kGeoDoubles, geo_bytes, bar);
+        bulk_g2s(smem_u32(geo_base + b * geo_buffer_bytes()), it.geo + c0 * kGeoDoubles, geo_bytes, bar);
         if (P.bulk) {
-            const unsigned char *src = reinterpret_cast<const unsigned char *>(P.amps) + c0 * P.amp_stride * P.elem;
+            const unsigned char *src = it.amps + c0 * P.amp_stride * P.elem;
             const uint32_t dst = smem_u32(amp_base + b * amp_bytes);
             for (int i = 0; i < rows; ++i)
                 bulk_g2s(dst + i * row_bytes, src + (int64_t)i * P.amp_stride * P.elem, (uint32_t)row_bytes, bar);
@@ -425,7 +443,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     // inside it form a prefix.
     auto build_records = [&](int64_t k, int b) {
         const int64_t c0 = k * C;
-        const int cmax = (int)min((int64_t)C, P.n_traces - c0);
+        const int cmax = (int)min((int64_t)C, it.n_traces - c0);
         if (warp < PB) {
             const int q = warp, c = lane;
             const double *geo = reinterpret_cast<const double *>(geo_base + b * geo_buffer_bytes());
@@ -497,7 +515,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
         }
         if (!P.bulk) {   // amplitude rows not 16-byte aligned: plain cooperative copy
             unsigned char *dst = amp_base + b * amp_bytes;
-            const unsigned char *src = reinterpret_cast<const unsigned char *>(P.amps);
+            const unsigned char *src = it.amps;
             for (int e = tid; e < cmax * P.ns; e += kThreads) {
                 const int rr = e / P.ns, ii = e - rr * P.ns;
                 const int64_t gi = (c0 + rr) * P.amp_stride + ii;
@@ -521,30 +539,35 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                 float &a = s_acc[(q * R + r) * kThreads + tid];
                 if (p >= 0 && t < P.nt && a != 0.f) {
                     const int64_t idx = (int64_t)p * P.nt + t;
-                    if (P.image_f32) reinterpret_cast<float *>(P.image)[idx] += a;
-                    else reinterpret_cast<double *>(P.image)[idx] += (double)a;
+                    if (P.image_f32) reinterpret_cast<float *>(it.image)[idx] += a;
+                    else reinterpret_cast<double *>(it.image)[idx] += (double)a;
                 }
                 a = 0.f;
             }
         }
     };
 
-    __syncthreads();   // barriers initialised, pillars known
+    __syncthreads();   // pillars known
+    // chunk k of this item is the CTA's chunk g = chunk_base + k: buffer g & 1,
+    // mbarrier phase parity (g >> 1) & 1
+    const int b0 = (int)(chunk_base & 1);
     if (tid == 0) {
-        if (n_chunks > 0) issue_chunk(0, 0);
-        if (n_chunks > 1) issue_chunk(1, 1);
+        if (chunk_base > 0) fence_proxy_async();   // the previous item's reads of the buffers
+        if (n_chunks > 0) issue_chunk(0, b0);
+        if (n_chunks > 1) issue_chunk(1, b0 ^ 1);
     }
     bool aborted = false;
     if (n_chunks > 0) {
-        const bool ok = mbar_wait(bar0, 0);
+        const bool ok = mbar_wait(b0 ? bar1 : bar0, (uint32_t)((chunk_base >> 1) & 1));
         if (__syncthreads_or(!ok)) aborted = true;
-        else build_records(0, 0);
+        else build_records(0, b0);
     }
     __syncthreads();
 
     for (int64_t k = 0; k < n_chunks && !aborted; ++k) {
         const int64_t c0 = k * C;
-        const int buf = (int)(k & 1);
+        const int64_t g = chunk_base + k;
+        const int buf = (int)(g & 1);
         const float4 *recA = reinterpret_cast<const float4 *>(rec_base + buf * REC_BYTES);
         const unsigned char *ampb = amp_base + buf * amp_bytes;
 
@@ -580,7 +603,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                     bool act = A.x <= s.ap;
                     const int slot = __float_as_int(A.w);
                     if (HARD && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
-                        act = !exact_outside_aperture(Pg, c0 + slot, p, t, s_ox[q], s_oy[q]);
+                        act = !exact_outside_aperture(Pg, it.trace0 + c0 + slot, p, t, s_ox[q], s_oy[q]);
                     float T, f;
                     int i0;
                     bool ok;
@@ -604,7 +627,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
                         const bool fast_ok = sidx >= sg_lo && sidx <= sg_hi;
                         const bool band = act && !fast_ok && sidx >= sr_lo && sidx <= sr_hi;
                         if constexpr (SLOW) {   // re-decide the guard band in FP64
-                            ok = band && exact_sample_ok<TT>(Pg, c0 + slot, p, t, s_ox[q], s_oy[q]);
+                            ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + slot, p, t, s_ox[q], s_oy[q]);
                             sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
                         } else {
                             ok = act && fast_ok;
@@ -661,7 +684,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
         bool timeout = false;
         if (k + 1 < n_chunks) {
             const int nb = buf ^ 1;
-            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((k + 1) >> 1) & 1));
+            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1));
             if (!timeout) build_records(k + 1, nb);
         }
         if ((k + 1) % flush_every == 0) flush();
@@ -675,6 +698,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
         }
     }
 
+    chunk_base += n_chunks;
     if (aborted) {
         // a copy never completed: report, drain what may still be in flight, leave
         if (tid == 0) {
@@ -685,12 +709,12 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
             mbar_wait(bar1, 1);
         }
         __syncthreads();
-        return;
+        return false;
     }
 
     // ---------------- epilogue: image += the last partials; fold += count
     flush();
-    if (P.fold && P.fold3d) {
+    if (it.fold && P.fold3d) {
 #pragma unroll
         for (int q = 0; q < PB; ++q) {
             const int p = s_pid[q];
@@ -699,13 +723,84 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int t = t_lane + r * kThreads;
-                if (t < P.nt) P.fold[(int64_t)p * P.nt + t] += cnt;
+                if (t < P.nt) it.fold[(int64_t)p * P.nt + t] += cnt;
             }
         }
     }
-    if (P.fold && !P.fold3d && blockIdx.y == 0 && tid < PB) {
+    if (it.fold && !P.fold3d && it.tblock == 0 && tid < PB) {
         const int p = s_pid[tid];
-        if (p >= 0) P.fold[p] += s_fold[tid];
+        if (p >= 0) it.fold[p] += s_fold[tid];
+    }
+    return true;
+}
+
+// Initialises the two staging mbarriers of a CTA.
+__device__ __forceinline__ void init_barriers(CtaShared &sh) {
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&sh.bar[0]), 1);
+        mbar_init(smem_u32(&sh.bar[1]), 1);
+        fence_barrier_init();
+    }
+}
+
+// One CTA per (pillar block, time block) of one tile.
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+__global__ void __launch_bounds__(kThreads, 1)
+migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
+    static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
+    static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ CtaShared sh;
+    init_barriers(sh);
+    Item it;
+    it.amps = reinterpret_cast<const unsigned char *>(P.amps);
+    it.geo = P.geo;
+    it.trace0 = 0;
+    it.n_traces = P.n_traces;
+    it.image = P.image;
+    it.fold = P.fold;
+    it.pbx = blockIdx.x / P.n_pblk_y;
+    it.pby = blockIdx.x - it.pbx * P.n_pblk_y;
+    it.tblock = blockIdx.y;
+    int64_t chunk_base = 0;
+    migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base);
+}
+
+// Persistent form for many outputs (offset bins): one CTA per SM fetches
+// items from a work counter; items of the bins with the most traces come
+// first (the host orders `bins`), so uneven bins balance.
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+__global__ void __launch_bounds__(kThreads, 1)
+migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const BinWork *__restrict__ bins,
+                          int n_bins, unsigned long long *work_counter) {
+    static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ CtaShared sh;
+    init_barriers(sh);
+    const int n_pblk_x = (P.nx + P.px - 1) / P.px;
+    const long long per_bin = (long long)n_pblk_x * P.n_pblk_y * P.n_tblk;
+    const long long n_items = per_bin * n_bins;
+    int64_t chunk_base = 0;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) sh.item = (long long)atomicAdd(work_counter, 1ull);
+        __syncthreads();
+        const long long item = sh.item;
+        if (item >= n_items) break;
+        const BinWork &bw = bins[item / per_bin];
+        long long rem = item - (item / per_bin) * per_bin;
+        Item it;
+        it.tblock = (int)(rem % P.n_tblk);
+        rem /= P.n_tblk;
+        it.pbx = (int)(rem / P.n_pblk_y);
+        it.pby = (int)(rem - (long long)it.pbx * P.n_pblk_y);
+        it.trace0 = bw.trace0;
+        it.n_traces = bw.n_traces;
+        it.amps = reinterpret_cast<const unsigned char *>(P.amps) + bw.trace0 * P.amp_stride * P.elem;
+        it.geo = P.geo + bw.trace0 * kGeoDoubles;
+        it.image = bw.image;
+        it.fold = bw.fold;
+        if (!migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base)) break;
     }
 }
 

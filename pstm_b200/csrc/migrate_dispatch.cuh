@@ -2,34 +2,58 @@
 // kind is instantiated in its own translation unit (migrate_k<kind>.cu) so
 // that they compile in parallel.
 #pragma once
+#include "launch.h"
 #include "migrate.cuh"
 
 namespace pstm {
 
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
-static cudaError_t launch_w(const KParams &P, const KParams *Pg, dim3 grid, size_t smem, cudaStream_t st) {
-    auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
-    static size_t configured = 0;   // dynamic shared memory opt-in, per instantiation
-    if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
+static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L) {
+    if (!L.bins) {
+        auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
+        static size_t configured = 0;   // dynamic shared memory opt-in, per instantiation
+        if (L.smem > configured) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+            if (e != cudaSuccess) return e;
+            configured = L.smem;
+        }
+        kern<<<L.grid, kThreads, L.smem, L.stream>>>(P, Pg);
+        return cudaGetLastError();
     }
-    kern<<<grid, kThreads, smem, st>>>(P, Pg);
+    auto kern = migrate_persistent_kernel<TT, AMP, VEL3D, EXACT, W2>;
+    static size_t configured = 0;
+    if (L.smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        if (e != cudaSuccess) return e;
+        configured = L.smem;
+    }
+    unsigned ctas = L.grid.x;
+    if (ctas == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, L.smem);
+        if (e != cudaSuccess) return e;
+        ctas = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+    }
+    if (L.configure_only) {
+        if (L.ctas_out) *L.ctas_out = ctas;
+        return cudaSuccess;
+    }
+    kern<<<ctas, kThreads, L.smem, L.stream>>>(P, Pg, L.bins, L.n_bins, L.counter);
     return cudaGetLastError();
 }
 
 template <int TT, int AMP, bool VEL3D, bool EXACT>
-static cudaError_t launch_one(const KParams &P, const KParams *Pg, dim3 grid, size_t smem, cudaStream_t st) {
-    if (P.spreading && P.obliquity) return launch_w<TT, AMP, VEL3D, EXACT, true>(P, Pg, grid, smem, st);
-    return launch_w<TT, AMP, VEL3D, EXACT, false>(P, Pg, grid, smem, st);
+static cudaError_t launch_one(const KParams &P, const KParams *Pg, const Launch &L) {
+    if (P.spreading && P.obliquity) return launch_w<TT, AMP, VEL3D, EXACT, true>(P, Pg, L);
+    return launch_w<TT, AMP, VEL3D, EXACT, false>(P, Pg, L);
 }
 
 template <int TT, bool EXACT>
-static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, bool vel3d, dim3 grid, size_t smem,
-                               cudaStream_t st) {
+static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, bool vel3d, const Launch &L) {
 #define PSTM_CASE(A_, V_) \
-    if (amp == A_ && vel3d == V_) return launch_one<TT, A_, V_, EXACT>(P, Pg, grid, smem, st);
+    if (amp == A_ && vel3d == V_) return launch_one<TT, A_, V_, EXACT>(P, Pg, L);
     PSTM_CASE(AMP_F32, false) PSTM_CASE(AMP_F32, true)
     PSTM_CASE(AMP_BF16, false) PSTM_CASE(AMP_BF16, true)
     PSTM_CASE(AMP_F16, false) PSTM_CASE(AMP_F16, true)
@@ -39,12 +63,11 @@ static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, boo
 
 // exact: FP64 sample index (straight rays only); otherwise FP32 traveltime.
 template <int TT>
-cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact, dim3 grid,
-                           size_t smem, cudaStream_t st) {
+cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact, const Launch &L) {
     if constexpr (TT == TT_STRAIGHT) {
-        if (exact) return launch_prec<TT, true>(P, Pg, amp, vel3d, grid, smem, st);
+        if (exact) return launch_prec<TT, true>(P, Pg, amp, vel3d, L);
     }
-    return launch_prec<TT, false>(P, Pg, amp, vel3d, grid, smem, st);
+    return launch_prec<TT, false>(P, Pg, amp, vel3d, L);
 }
 
 }  // namespace pstm

@@ -24,11 +24,10 @@
 
 #include "pstm_cuda.h"
 #include "kparams.h"
+#include "launch.h"
 #include "plan.h"
 
 namespace pstm {
-template <int TT>
-cudaError_t launch_migrate(const KParams &, const KParams *, int, bool, bool, dim3, size_t, cudaStream_t);
 void set_context_free_error(const std::string &msg);
 }  // namespace pstm
 
@@ -55,14 +54,6 @@ static_assert(kOffTab % 256 == 0 && kOffGeo % 256 == 0, "scratch regions must st
 // The scratch array.  Host code must not use the symbol as a pointer: it is a
 // host-side stand-in.  Its device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
-
-// Writes the launch parameters into the scratch array (the kernel's rare FP64
-// paths read them there); a kernel rather than a copy from host memory.
-__global__ void store_params(const KParams P) {
-    const unsigned *src = reinterpret_cast<const unsigned *>(&P);
-    unsigned *dst = reinterpret_cast<unsigned *>(g_scratch + kOffParams);
-    for (unsigned i = threadIdx.x; i < sizeof(KParams) / 4; i += blockDim.x) dst[i] = src[i];
-}
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
@@ -168,7 +159,9 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     if (blocks > 148 * 32) blocks = 148 * 32;
     pack_geometry<<<blocks, 256, 0, st>>>(P, reinterpret_cast<double *>(scratch + kOffGeo));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "pack_geometry launch");
-    store_params<<<1, 32, 0, st>>>(P);
+    // the launch parameters for the kernel's rare FP64 paths: written by a
+    // kernel rather than copied from host memory
+    store_params<<<1, 32, 0, st>>>(P, reinterpret_cast<KParams *>(scratch + kOffParams));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "store_params launch");
     const KParams *Pg = reinterpret_cast<const KParams *>(scratch + kOffParams);
 
@@ -177,14 +170,11 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     const int tb = kThreads * R;
     const int nblk_t = (out->nt + tb - 1) / tb;
     if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
-    dim3 grid((unsigned)nblk_p, (unsigned)nblk_t);
-    const int amp = tr->amp_dtype;
-    switch (prm->traveltime) {
-    case PSTM_TT_STRAIGHT: e = launch_migrate<TT_STRAIGHT>(P, Pg, amp, per_pillar, exact, grid, smem, st); break;
-    case PSTM_TT_CURVED: e = launch_migrate<TT_CURVED>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    case PSTM_TT_VTI: e = launch_migrate<TT_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    default: e = launch_migrate<TT_CURVED_VTI>(P, Pg, amp, per_pillar, false, grid, smem, st); break;
-    }
+    Launch L;
+    L.grid = dim3((unsigned)nblk_p, (unsigned)nblk_t);
+    L.smem = smem;
+    L.stream = st;
+    e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, exact, L);
     if (e != cudaSuccess) return cuda_fail(e, "migrate kernel launch");
     return PSTM_OK;
 }

@@ -148,7 +148,7 @@ inline void choose_shape(int nt, int force_r, int force_pb, int &R, int &PB) {
 // Staging plan: row pitch, TMA eligibility, traces per chunk and the dynamic
 // shared memory of one CTA.  Returns false when a row does not fit.
 inline bool plan_staging(KParams &P, const pstm_traces_desc *tr, const pstm_params *prm, int PB, int R,
-                         int smem_optin, size_t &smem) {
+                         int smem_optin, size_t &smem, int force_chunk = 0) {
     const int eb = P.elem;
     const int per16 = 16 / eb;
     const int pitch = (tr->n_samples + per16 - 1) / per16 * per16;
@@ -162,11 +162,13 @@ inline bool plan_staging(KParams &P, const pstm_traces_desc *tr, const pstm_para
     const size_t budget = (size_t)smem_optin > fixed + static_bytes ? smem_optin - fixed - static_bytes : 0;
     int chunk = (int)(budget / (2 * (size_t)pitch * eb));
     if (chunk > kMaxChunk) chunk = kMaxChunk;
+    if (force_chunk >= 1 && force_chunk < chunk) chunk = force_chunk;   // tuning: a shallower panel
     if (chunk < 1) return false;
     P.chunk = chunk;
     P.pb = PB;
     P.r_per_lane = R;
     P.flush_every = 16;
+    P.n_tblk = (P.nt + kThreads * R - 1) / (kThreads * R);
     smem = 2 * (size_t)chunk * pitch * eb + fixed;
     return true;
 }

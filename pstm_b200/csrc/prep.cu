@@ -1,4 +1,5 @@
 // prep.cu -- per-(pillar|0, time) tables for the gather kernel.
+#include "launch.h"
 #include "migrate.cuh"
 
 namespace pstm {
@@ -62,6 +63,21 @@ __global__ void pack_geometry(const KParams P, double *geo) {
         g[6] = P.w ? P.w[i] : 1.0;
         g[7] = 0.0;
     }
+}
+
+// Writes the launch parameters to device memory (the kernels' rare FP64 paths
+// read them there).  A kernel rather than a copy from host memory, so that it
+// can be captured in a CUDA graph and needs no staging buffer.
+__global__ void store_params(const KParams P, KParams *dst) {
+    const unsigned *src = reinterpret_cast<const unsigned *>(&P);
+    unsigned *d = reinterpret_cast<unsigned *>(dst);
+    for (unsigned i = threadIdx.x; i < sizeof(KParams) / 4; i += blockDim.x) d[i] = src[i];
+}
+
+// Writes up to kBinsPerStore work descriptors of the persistent form to
+// device memory; their values travel as kernel parameters (graph-capturable).
+__global__ void store_bins(const BinStore b, BinWork *dst) {
+    for (int i = threadIdx.x; i < b.count; i += blockDim.x) dst[b.first + i] = b.w[i];
 }
 
 }  // namespace pstm

@@ -124,6 +124,16 @@ class CudaKernel:
     def migrate_tile_curved_vti(self, traces, output, velocity, config=None) -> KernelMetrics:
         return self._migrate(traces, output, velocity, config, nat.TT_CURVED_VTI)
 
+    def migrate_bins(self, traces, bins, geometry, velocity, config=None,
+                     kernel_type: str = "straight_ray") -> KernelMetrics:
+        """The batched form; see :func:`migrate_bins`."""
+        return migrate_bins(self, traces, bins, geometry, velocity, config, kernel_type)
+
+    def autotune_bins(self, traces, bins, geometry, velocity, config=None, kernel_type: str = "straight_ray",
+                      pairs_per_candidate: int = 0) -> dict:
+        """The autotuner of the batched form; see :func:`autotune_bins`."""
+        return autotune_bins(self, traces, bins, geometry, velocity, config, kernel_type, pairs_per_candidate)
+
     def synchronize(self) -> None:
         if self._ctx is not None:
             nat.check(self._lib.pstm_cuda_synchronize(self._ctx), self._ctx, self._lib)
@@ -145,7 +155,7 @@ class CudaKernel:
     def context(self):
         return self._ctx
 
-    def _params(self, cfg, tt: int, keep: list, eta_override=None) -> nat.Params:
+    def _params(self, cfg, tt: int, keep: list, eta_override=None, devs: list | None = None) -> nat.Params:
         p = nat.Params()
         p.max_aperture_m = float(cfg.max_aperture_m)
         p.min_aperture_m = float(cfg.min_aperture_m)
@@ -165,7 +175,9 @@ class CudaKernel:
         p.precision = self._precision
         eta = eta_override if eta_override is not None else getattr(cfg, "vti_eta_array", None)
         if eta is not None and tt in (nat.TT_VTI, nat.TT_CURVED_VTI):
-            ptr, _ = self._arr(eta, np.float64, keep)
+            ptr, on_dev = self._arr(eta, np.float64, keep)
+            if devs is not None:
+                devs.append(on_dev)
             p.eta = ptr
             p.eta_is_3d = 0 if len(eta.shape) == 1 else 1
         return p
@@ -246,24 +258,15 @@ class CudaKernel:
         keep.append(v)
         return v.ctypes.data, is3d, False
 
-    def _migrate(self, traces, output, velocity, config, tt: int) -> KernelMetrics:
-        if self._ctx is None or self._config is None:
-            raise RuntimeError("Kernel not initialized")
-        cfg = config if config is not None else self._config
-        t_start = time.perf_counter()
-        keep: list = []
-        nx, ny, nt = len(output.x_axis), len(output.y_axis), len(output.t_axis_ms)
-        ntr = int(traces.amplitudes.shape[0])
-        ns = int(traces.amplitudes.shape[1])
-
+    def _trace_desc(self, traces, keep: list, devs: list) -> nat.TracesDesc:
         amp_ptr, amp_code, amp_stride, amp_dev = self._amplitudes(traces.amplitudes, keep)
         td = nat.TracesDesc()
         td.amplitudes = amp_ptr
         td.amp_dtype = amp_code
-        td.n_samples = ns
-        td.n_traces = ntr
+        td.n_samples = int(traces.amplitudes.shape[1])
+        td.n_traces = int(traces.amplitudes.shape[0])
         td.amp_row_stride = amp_stride
-        devs = [amp_dev]
+        devs.append(amp_dev)
         for name in ("source_x", "source_y", "receiver_x", "receiver_y", "midpoint_x", "midpoint_y"):
             ptr, d = self._arr(getattr(traces, name), np.float64, keep)
             setattr(td, name, ptr)
@@ -275,6 +278,31 @@ class CudaKernel:
             devs.append(d)
         td.sample_rate_ms = float(traces.sample_rate_ms)
         td.start_time_ms = float(traces.start_time_ms)
+        return td
+
+    def _output_axes(self, output, od: nat.OutputDesc, keep: list, devs: list) -> None:
+        od.nx, od.ny, od.nt = len(output.x_axis), len(output.y_axis), len(output.t_axis_ms)
+        od.x_axis, d1 = self._arr(output.x_axis, np.float64, keep)
+        od.y_axis, d2 = self._arr(output.y_axis, np.float64, keep)
+        od.t_axis_ms, d3 = self._arr(output.t_axis_ms, np.float64, keep)
+        devs += [d1, d2, d3]
+        xg, yg = getattr(output, "x_grid", None), getattr(output, "y_grid", None)
+        if xg is not None and yg is not None:
+            od.x_grid, d4 = self._arr(xg, np.float64, keep)
+            od.y_grid, d5 = self._arr(yg, np.float64, keep)
+            devs += [d4, d5]
+
+    def _migrate(self, traces, output, velocity, config, tt: int) -> KernelMetrics:
+        if self._ctx is None or self._config is None:
+            raise RuntimeError("Kernel not initialized")
+        cfg = config if config is not None else self._config
+        t_start = time.perf_counter()
+        keep: list = []
+        nx, ny, nt = len(output.x_axis), len(output.y_axis), len(output.t_axis_ms)
+        ntr = int(traces.amplitudes.shape[0])
+
+        devs: list = []
+        td = self._trace_desc(traces, keep, devs)
 
         od = nat.OutputDesc()
         img = output.image
@@ -305,21 +333,12 @@ class CudaKernel:
                 od.fold = fold.ctypes.data
                 devs.append(False)
             od.fold_is_3d = 1 if len(fold.shape) == 3 else 0
-        od.nx, od.ny, od.nt = nx, ny, nt
-        od.x_axis, d1 = self._arr(output.x_axis, np.float64, keep)
-        od.y_axis, d2 = self._arr(output.y_axis, np.float64, keep)
-        od.t_axis_ms, d3 = self._arr(output.t_axis_ms, np.float64, keep)
-        devs += [d1, d2, d3]
-        xg, yg = getattr(output, "x_grid", None), getattr(output, "y_grid", None)
-        if xg is not None and yg is not None:
-            od.x_grid, d4 = self._arr(xg, np.float64, keep)
-            od.y_grid, d5 = self._arr(yg, np.float64, keep)
-            devs += [d4, d5]
+        self._output_axes(output, od, keep, devs)
 
         vd = nat.VelocityDesc()
         vd.vrms, vd.is_3d, dv = self._velocity(velocity, output, nx, ny, nt, keep)
         devs.append(dv)
-        prm = self._params(cfg, tt, keep)
+        prm = self._params(cfg, tt, keep, devs=devs)
 
         on_dev = all(devs)
         if any(devs) and not on_dev:
@@ -336,6 +355,108 @@ class CudaKernel:
         nat.check(rc, self._ctx, self._lib)
         return KernelMetrics(n_traces_processed=ntr, n_samples_output=nx * ny * nt,
                              compute_time_s=time.perf_counter() - t_start)
+
+
+class Bin:
+    """One output of the batched form: traces [trace_begin, trace_begin +
+    n_traces) of the batch's trace block, migrated into its own image (and
+    fold).  Reference: one gather bin of ``executor.py:960-975``."""
+
+    def __init__(self, trace_begin: int, n_traces: int, image, fold=None):
+        self.trace_begin = int(trace_begin)
+        self.n_traces = int(n_traces)
+        self.image = image
+        self.fold = fold
+
+
+def _batch_descs(kernel: "CudaKernel", traces, bins, geometry, velocity, config, kernel_type: str):
+    """Descriptors of a batched call (device tensors only)."""
+    if kernel._ctx is None or kernel._config is None:
+        raise RuntimeError("Kernel not initialized")
+    if kernel_type not in _TT_BY_TYPE:
+        raise ValueError(f"unknown kernel_type {kernel_type!r}")
+    import torch
+    cfg = config if config is not None else kernel._config
+    keep: list = []
+    devs: list = []
+    td = kernel._trace_desc(traces, keep, devs)
+    od = nat.OutputDesc()
+    kernel._output_axes(geometry, od, keep, devs)
+    nx, ny, nt = od.nx, od.ny, od.nt
+    vd = nat.VelocityDesc()
+    vd.vrms, vd.is_3d, dv = kernel._velocity(velocity, geometry, nx, ny, nt, keep)
+    devs.append(dv)
+    prm = kernel._params(cfg, _TT_BY_TYPE[kernel_type], keep, devs=devs)
+    if not all(devs):
+        raise ValueError("the batched form takes CUDA tensors only (traces, axes, velocity and eta)")
+    arr = (nat.BinDesc * max(1, len(bins)))()
+    img_dtype = None
+    fold3 = None
+    for i, b in enumerate(bins):
+        img = b.image
+        if not _is_torch_cuda(img) or not img.is_contiguous() or img.dtype not in (torch.float64, torch.float32):
+            raise ValueError(f"bin {i}: image must be a contiguous float64/float32 CUDA tensor")
+        if tuple(img.shape) != (nx, ny, nt):
+            raise ValueError(f"bin {i}: image shape {tuple(img.shape)} != {(nx, ny, nt)}")
+        if img_dtype is None:
+            img_dtype = img.dtype
+        elif img.dtype != img_dtype:
+            raise ValueError("all bins' images must have one dtype")
+        arr[i].trace_begin, arr[i].n_traces, arr[i].image = b.trace_begin, b.n_traces, img.data_ptr()
+        if b.fold is not None:
+            f = b.fold
+            if not _is_torch_cuda(f) or f.dtype != torch.int32 or not f.is_contiguous():
+                raise ValueError(f"bin {i}: fold must be a contiguous int32 CUDA tensor")
+            shape = (nx, ny, nt) if len(f.shape) == 3 else (nx, ny)
+            if tuple(f.shape) != shape or (fold3 is not None and fold3 != (len(shape) == 3)):
+                raise ValueError(f"bin {i}: fold must be (nx, ny, nt) or (nx, ny), the same for every bin")
+            fold3 = len(shape) == 3
+            arr[i].fold = f.data_ptr()
+    od.fold_is_3d = 1 if fold3 else 0
+    od.image_dtype = nat.IMAGE_F32 if img_dtype == torch.float32 else nat.IMAGE_F64
+    keep.append(arr)
+    return td, od, vd, prm, arr, keep
+
+
+def migrate_bins(kernel: "CudaKernel", traces, bins, geometry, velocity, config=None,
+                 kernel_type: str = "straight_ray") -> KernelMetrics:
+    """Migrate many bins sharing one tile geometry in ONE persistent launch
+    (replayed from a CUDA graph while the arguments repeat).
+
+    ``traces`` holds every bin's traces (CUDA tensors), ``bins`` is a list of
+    :class:`Bin`, ``geometry`` gives the tile axes (an ``OutputTile``; its own
+    image is not used).  Replaces the executor's per-bin loop of
+    ``migrate_tile`` calls (``executor.py:960-975``).  Asynchronous on the
+    current torch stream; ``kernel.synchronize()`` reports kernel-side errors.
+    """
+    import torch
+    t0 = time.perf_counter()
+    td, od, vd, prm, arr, keep = _batch_descs(kernel, traces, bins, geometry, velocity, config, kernel_type)
+    stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+    rc = kernel._lib.pstm_cuda_migrate_bins_dev(kernel._ctx, ctypes.byref(td), ctypes.byref(od), ctypes.byref(vd),
+                                                ctypes.byref(prm), arr, len(bins), ctypes.c_void_p(stream))
+    nat.check(rc, kernel._ctx, kernel._lib)
+    return KernelMetrics(n_traces_processed=sum(b.n_traces for b in bins),
+                         n_samples_output=od.nx * od.ny * od.nt * len(bins),
+                         compute_time_s=time.perf_counter() - t0)
+
+
+def autotune_bins(kernel: "CudaKernel", traces, bins, geometry, velocity, config=None,
+                  kernel_type: str = "straight_ray", pairs_per_candidate: int = 0) -> dict:
+    """Time the candidate launch shapes of the batched form on a sample of
+    this batch and keep the fastest in the kernel's context (later
+    :func:`migrate_bins` calls of the same workload class use it)."""
+    import torch
+    torch.cuda.synchronize()
+    td, od, vd, prm, arr, keep = _batch_descs(kernel, traces, bins, geometry, velocity, config, kernel_type)
+    res = nat.TuneResult()
+    rc = kernel._lib.pstm_cuda_autotune_bins(kernel._ctx, ctypes.byref(td), ctypes.byref(od), ctypes.byref(vd),
+                                             ctypes.byref(prm), arr, len(bins), int(pairs_per_candidate),
+                                             ctypes.byref(res))
+    nat.check(rc, kernel._ctx, kernel._lib)
+    return {"pillars_per_cta": res.pillars_per_cta, "times_per_lane": res.times_per_lane,
+            "traces_per_chunk": res.traces_per_chunk, "n_candidates": res.n_candidates,
+            "best_ms": res.best_ms, "default_ms": res.default_ms}
 
 
 def create_cuda_kernel(**kw) -> CudaKernel:

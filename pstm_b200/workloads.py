@@ -8,6 +8,10 @@ diffraction responses plus Gaussian noise, generated from a fixed seed.
   (offset <= 2 km), diffractors (800,800,0.6 s), (500,1100,1.0 s),
   (1200,400,1.4 s) in v = 2000 m/s, SNR 10; aperture 1000 m, dip 60 deg,
   weights on, AA off.
+* ``binned_survey``  the batched case: traces sorted into common-offset bins
+  of equal width (40 bins over 0-4 km), the trace count of each bin drawn
+  lognormal between 5k and 200k (about 2M in all), midpoints uniform over the
+  patch, azimuths uniform; each bin is a contiguous range of the panel.
 * ``survey``   the larger cases (2-5): bins of 12.5 m, laterally varying
   v_rms(t,x,y) = (1500 + 2500 t/3 s)(1 + 0.05 G(x,y)), G a unit-variance
   Gaussian-smoothed field with a 300 m correlation length, eta(t0) rising
@@ -238,3 +242,56 @@ def survey_device(n_traces: int, nx: int, ny: int, nt: int, dt_ms: float, ns: in
     amps = diffraction_panel_torch(sv.s, sv.r, diffr, lambda t0: 1500.0 + 2500.0 * t0 / 3.0, ns,
                                    dt_ms / 1000.0, seed + 200, device=device, dtype=dtype)
     return sv, amps
+
+
+# ----------------------------------------------------------------- offset bins
+def offset_bin_counts(n_bins: int, lo: int, hi: int, total: int, seed: int) -> np.ndarray:
+    """Trace counts per bin: lognormal between lo and hi, scaled to about `total`."""
+    rng = np.random.default_rng(seed)
+    mu = 0.5 * (np.log(lo) + np.log(hi))
+    sigma = (np.log(hi) - np.log(lo)) / 4.0
+    c = np.clip(np.exp(rng.normal(mu, sigma, n_bins)), lo, hi)
+    c = np.clip(c * (total / c.sum()), lo, hi)
+    return np.rint(c).astype(np.int64)
+
+
+@dataclass
+class BinnedSurvey:
+    survey: Survey
+    starts: np.ndarray      # first trace of each bin
+    counts: np.ndarray      # traces of each bin
+    bin_width_m: float
+    amps_device: object = None   # torch tensor when generated on the device
+
+
+def binned_survey(counts, nx: int, ny: int, nt: int, dt_ms: float, ns: int, dx: float = 12.5,
+                  bin_width_m: float = 100.0, n_diffractors: int = 6, seed: int = 11,
+                  device=None, dtype=None) -> BinnedSurvey:
+    """Traces of common-offset bins [b w, (b+1) w), bin after bin, over an
+    nx*dx x ny*dx patch with the ``survey`` velocity.  With ``device`` the
+    amplitudes are generated there (``amps_device``), else on the host."""
+    counts = np.asarray(counts, dtype=np.int64)
+    rng = np.random.default_rng(seed)
+    n = int(counts.sum())
+    h = np.concatenate([rng.uniform(b * bin_width_m, (b + 1) * bin_width_m, int(c))
+                        for b, c in enumerate(counts)]) if n else np.zeros(0)
+    az = rng.uniform(0.0, 2.0 * np.pi, n)
+    m = np.stack([rng.uniform(0.0, nx * dx, n), rng.uniform(0.0, ny * dx, n)], axis=1)
+    d = 0.5 * h[:, None] * np.stack([np.cos(az), np.sin(az)], axis=1)
+    s, r = m - d, m + d
+    G = lateral_field(nx, ny, dx, 300.0, seed + 1)
+    tmax = (nt - 1) * dt_ms / 1000.0
+    diffr = [(rng.uniform(0.2, 0.8) * nx * dx, rng.uniform(0.2, 0.8) * ny * dx,
+              rng.uniform(0.25, 0.7) * tmax) for _ in range(n_diffractors)]
+    v_of_t0 = lambda t0: 1500.0 + 2500.0 * t0 / 3.0
+    amps, amps_dev = None, None
+    if device is not None:
+        amps_dev = diffraction_panel_torch(s, r, diffr, v_of_t0, ns, dt_ms / 1000.0, seed + 200,
+                                           device=device, dtype=dtype)
+    else:
+        amps = diffraction_panel(s, r, diffr, v_of_t0, ns, dt_ms / 1000.0, rng, dtype=dtype or np.float32)
+    sv = Survey(s=s, r=r, amps=amps, dt_ms=dt_ms, x_axis=np.arange(nx) * dx, y_axis=np.arange(ny) * dx,
+                t_axis_ms=np.arange(nt) * dt_ms, G=G, dx=dx)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64)
+    return BinnedSurvey(sv, starts, counts, bin_width_m, amps_dev)
+

@@ -56,6 +56,8 @@ def test_null_context_errors_without_gpu(lib_path):
     assert b"not initialized" in L.pstm_cuda_last_error(None)
     rc = L.pstm_cuda_migrate_tile_host(None, None, None, None, None)
     assert rc == nat.ERR_NOT_INITIALIZED
+    assert L.pstm_cuda_migrate_bins_dev(None, None, None, None, None, None, 0, None) == nat.ERR_NOT_INITIALIZED
+    assert L.pstm_cuda_autotune_bins(None, None, None, None, None, None, 0, 0, None) == nat.ERR_NOT_INITIALIZED
     with pytest.raises(RuntimeError, match="not initialized"):
         nat.check(rc, None, L)
 
@@ -65,7 +67,8 @@ def _c_layout(tmp_path):
     from pstm_b200 import _native as nat
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pstm_cuda.h"', 'int main(void){']
     for cname, cls in (("pstm_traces_desc", nat.TracesDesc), ("pstm_output_desc", nat.OutputDesc),
-                       ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params)):
+                       ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params),
+                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult)):
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for f, _ in cls._fields_:
             lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
@@ -82,7 +85,8 @@ def test_ctypes_structs_match_header_layout(tmp_path):
     from pstm_b200 import _native as nat
     lay = _c_layout(tmp_path)
     for cname, cls in (("pstm_traces_desc", nat.TracesDesc), ("pstm_output_desc", nat.OutputDesc),
-                       ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params)):
+                       ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params),
+                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult)):
         assert lay[(cname, "size")] == ctypes.sizeof(cls), cname
         for f, _ in cls._fields_:
             assert lay[(cname, f)] == getattr(cls, f).offset, (cname, f)
