@@ -68,6 +68,7 @@ struct KParams {
     int32_t flush_every;         // chunks between flushes of the FP32 partials
     int32_t exact_units;         // weights' time unit: 1 = samples (EXACT), 0 = seconds
     int32_t curved_kind;         // curved-ray traveltime (its T can be ~0 at t0 > 0)
+    int32_t t0_zero_exact;       // at t0 = 0 every pair has T = 0 exactly in FP64 (VTI; curved, k != 0)
     const double *eta;           // nullable (FP64, exact paths)
     double eta_const;
 

@@ -13,7 +13,7 @@ namespace pstm {
 // blocks, time blocks)) or the persistent form over `n_bins` outputs (grid.x
 // CTAs; grid.x == 0 asks for one CTA per SM times the occupancy).
 struct Launch {
-    dim3 grid;
+    dim3 grid = dim3(0, 1, 1);   // dim3's own default is (1, 1, 1)
     size_t smem = 0;
     cudaStream_t stream = nullptr;
     const BinWork *bins = nullptr;

@@ -131,6 +131,7 @@ struct TimeState {
     float tguard;          // 1 ms in the unit of T
     float vz, vz2, ivwc;   // curved: velocity at image depth, 1/vz
     bool tzero;
+    bool tz, tz_in;        // t0 = 0 with T = 0 exactly for every pair; its sample index inside the trace
     double A;              // EXACT: (t0 / (2 dt))^2 (at least 1e-20)
 };
 
@@ -157,6 +158,8 @@ __device__ __forceinline__ void load_states(const KParams &P, int p, int t, Time
     ts.vz2 = b.y;
     ts.ivwc = b.z;
     ts.tzero = b.w != 0.f;
+    ts.tz = b.w >= 2.f;
+    ts.tz_in = b.w == 2.f;
     ts.A = EXACT ? P.ttimeA[tc] : 0.0;
     const int64_t ti = (P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc;
     const float4 tab = P.ttab[ti];
@@ -591,7 +594,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 const float tmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(tsl)));
                 const int n = __popc(__ballot_sync(0xffffffffu, dl <= apw));
                 const int n0 = min(n, __popc(__ballot_sync(0xffffffffu, dl <= tmin)));
-                bool pend = false;   // FP32 path: some pair lies in a trace-end guard band
+                unsigned pmask = 0u;   // FP32 path: records with a pair in a trace-end guard band
 
                 // contribution of record c (slot in the sorted order) to this lane's time
                 auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c) -> float {
@@ -623,15 +626,18 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
                         if constexpr (HAS_C) Cc = reinterpret_cast<const float4 *>(recA + 2 * RECS)[ri];
                         T = traveltime<TT>(P, ts, s, B, Cc);
+                        if constexpr (TT != TT_STRAIGHT) T = ts.tz ? 0.f : T;
                         float sidx = fmaf(T, s_scale, s_offset);
-                        const bool fast_ok = sidx >= sg_lo && sidx <= sg_hi;
-                        const bool band = act && !fast_ok && sidx >= sr_lo && sidx <= sr_hi;
+                        // T = 0 exactly: the FP64 decision is known per time, no guard band
+                        const bool fast_ok = ts.tz ? ts.tz_in : (sidx >= sg_lo && sidx <= sg_hi);
+                        const bool band = act && !fast_ok && !ts.tz && sidx >= sr_lo && sidx <= sr_hi;
+                        if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
                         if constexpr (SLOW) {   // re-decide the guard band in FP64
                             ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + slot, p, t, s_ox[q], s_oy[q]);
                             sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
                         } else {
                             ok = act && fast_ok;
-                            pend |= band;
+                            pmask |= band ? (1u << c) : 0u;
                         }
                         sidx = ok ? sidx : 0.f;
                         const float fl = __fadd_rd(sidx, 8388608.f);
@@ -671,9 +677,12 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
 #pragma unroll 2
                     for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{});
                 }
-                if constexpr (!EXACT) {
-                    if (__any_sync(0xffffffffu, pend)) {
-                        for (int c = 0; c < n; ++c) a += pair(c, Tr{}, Tr{}, Tr{});
+                if constexpr (!EXACT) {   // second pass over the flagged records only
+                    unsigned m = __reduce_or_sync(0xffffffffu, pmask);
+                    while (m) {
+                        const int c = __ffs(m) - 1;
+                        m &= m - 1u;
+                        a += pair(c, Tr{}, Tr{}, Tr{});
                     }
                 }
                 s_acc[(q * R + r) * kThreads + tid] += a;

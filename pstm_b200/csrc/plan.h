@@ -122,6 +122,10 @@ inline KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *o
     P.cr_kf = (float)prm->curved_k;
     P.cr_k_zero = std::fabs(prm->curved_k) < 1e-10 ? 1 : 0;
     P.cr_inv_k_ln2 = P.cr_k_zero ? 0.f : (float)(M_LN2 / prm->curved_k);
+    // VTI returns 2 t0/2 = 0 at t0 = 0; the curved leg of depth 0 is log(1) = 0 for k != 0
+    P.t0_zero_exact = (prm->traveltime == PSTM_TT_VTI ||
+                       ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) &&
+                        !P.cr_k_zero)) ? 1 : 0;
     P.compensated = prm->compensated ? 1 : 0;
 
     // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)

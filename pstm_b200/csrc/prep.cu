@@ -41,7 +41,14 @@ __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, doubl
             }
             ttime[2 * t] = make_float4((float)((t0 * 0.5) * (t0 * 0.5)), P.obliquity ? (float)(t0 / tu) : 1.f,
                                        small_t ? (float)tguard : -1.f, (float)tguard);
-            ttime[2 * t + 1] = make_float4(vz, vz2, ivwc, t0 > 0.0 ? 0.f : 1.f);
+            // w: 0 for t0 > 0; 1 for t0 = 0; 2 (3) for t0 = 0 where every T is exactly 0 and
+            // the FP64 sample index of T = 0 lies inside (outside) the trace
+            float w = 0.f;
+            if (!(t0 > 0.0)) {
+                const double s0 = (0.0 - P.tstart_s) / P.dt_s;
+                w = P.t0_zero_exact ? ((s0 >= 0.0 && s0 < (double)(P.ns - 1)) ? 2.f : 3.f) : 1.f;
+            }
+            ttime[2 * t + 1] = make_float4(vz, vz2, ivwc, w);
             const double th = t0 * 0.5 / P.dt_s;
             ttimeA[t] = fmax(th * th, 1e-20);   // keeps the FP64 legs > 0 at t0 = 0
         }
