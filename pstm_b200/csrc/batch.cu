@@ -373,7 +373,7 @@ int32_t pstm_cuda_autotune_bins(void *ctx, const pstm_traces_desc *traces, const
             continue;
         }
         if (rc) break;
-        if (s.chunk && s.chunk >= bp.P.chunk) continue;   // the same as the deepest panel
+        if (s.chunk && bp.P.chunk != s.chunk) continue;   // deeper than fits: the same as chunk 0
         float ms = 1e30f;
         for (int rep = 0; rep < 2 && rc == PSTM_OK; ++rep) {   // the first run warms up
             if ((e = cudaEventRecord(ev0, c->stream)) != cudaSuccess) {
