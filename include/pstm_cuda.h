@@ -222,6 +222,72 @@ int32_t pstm_cuda_autotune_bins(void *ctx, const pstm_traces_desc *traces, const
                                 const pstm_bin_desc *bins, int32_t n_bins, int64_t pairs_per_candidate,
                                 pstm_tune_result *result);
 
+/* ---------------------------------------------------------------- learned form
+ * A 7 -> 64 -> 64 -> 64 -> 1 SiLU network (BF16 weights on the tensor cores,
+ * FP32 accumulation) approximates the VTI or curved+VTI traveltime as the
+ * straight-ray DSR time plus a learned residual:
+ *   T = T_DSR(t0, h_s, h_r, v_rms) + out_scale * net((x - shift) * scale),
+ *   x = (t0 [s], dx_s, dy_s, dx_r, dy_r [m, output point minus source /
+ *   receiver], v_rms [m/s], eta).
+ * No reference counterpart: the reference evaluates the formulas only
+ * (pstm_anisotropic_vti.metal:103-148, pstm_curved_ray.metal:50-96). */
+typedef struct {
+    int32_t traveltime;           /* PSTM_TT_VTI or PSTM_TT_CURVED_VTI */
+    int32_t reserved;
+    double curved_v0, curved_k;   /* curved+VTI: V(z) = v0 + k z */
+    double t0_max_s;              /* t0 uniform in [0, t0_max_s] */
+    double h_max_m;               /* dx_s, dy_s, dx_r, dy_r uniform in [-h_max_m, h_max_m] */
+    double v_a, v_b, v_rel;       /* v_rms = (v_a + v_b t0) (1 + v_rel u), u uniform in [-1, 1] */
+    double eta_slope, eta_jitter, eta_max;   /* eta = clip(eta_slope t0 + eta_jitter u', 0, eta_max) */
+} pstm_surrogate_domain;
+
+typedef struct {
+    float shift[8], scale[8];     /* input normalisation (entries 7 unused) */
+    float out_scale;              /* seconds per unit of network output */
+    int32_t traveltime;           /* the kind the network was trained on */
+    const float *params;          /* device: pstm_cuda_surrogate_param_count() FP32 parameters */
+} pstm_surrogate;
+
+typedef struct {
+    float probe_max_ms;           /* largest |T_surrogate - T_exact| over the in-aperture probes */
+    float probe_rms_ms;
+    int32_t n_probe_used;         /* probes that fell inside their pair's aperture */
+    int32_t used_surrogate;       /* 1: the tile was migrated with the surrogate; 0: exact fallback */
+} pstm_learned_report;
+
+/* Number of FP32 parameters of the network (layout W1[64][7] b1 W2[64][64] b2 W3 b3 w4[64] b4). */
+int32_t pstm_cuda_surrogate_param_count(void);
+
+/* Seeded training/evaluation samples with exact FP64 targets: for sample
+ * first+j (j < n), raw[8 j .. 8 j + 6] = x (FP32) and residual[j] =
+ * T_exact - T_DSR (s); t_exact (nullable) gets T_exact.  Device pointers. */
+int32_t pstm_cuda_surrogate_samples(void *ctx, const pstm_surrogate_domain *domain, uint64_t seed, int64_t first,
+                                    int32_t n, float *raw, float *residual, double *t_exact, void *stream);
+
+/* Forward and backward pass over n samples: grads += d(mean squared error of
+ * the normalised residual)/d(params), loss_sum += the sum of squared errors. */
+int32_t pstm_cuda_surrogate_gradients(void *ctx, const pstm_surrogate *net, const float *raw, const float *residual,
+                                      int32_t n, float *grads, float *loss_sum, void *stream);
+
+/* One Adam step (beta 0.9 / 0.999, bias-corrected) on params; clears grads. */
+int32_t pstm_cuda_surrogate_adam(void *ctx, float *params, float *grads, float *m, float *v, int32_t step, float lr,
+                                 void *stream);
+
+/* Network residual (s) of n samples (raw as written by pstm_cuda_surrogate_samples). */
+int32_t pstm_cuda_surrogate_eval(void *ctx, const pstm_surrogate *net, const float *raw, int32_t n, float *residual,
+                                 void *stream);
+
+/* The learned form of pstm_cuda_migrate_tile_dev: n_probe random in-aperture
+ * (pillar, trace, time) pairs of the tile compare the surrogate with the exact
+ * FP64 traveltime; if the largest residual is at most max_residual_ms (0: the
+ * default 0.1 ms; negative: always use the surrogate) the tile is migrated
+ * with the surrogate traveltime, else with the exact kernel.  params->traveltime
+ * must be the network's kind.  Synchronises the stream once (the probe). */
+int32_t pstm_cuda_migrate_tile_learned_dev(void *ctx, const pstm_traces_desc *traces, const pstm_output_desc *output,
+                                           const pstm_velocity_desc *velocity, const pstm_params *params,
+                                           const pstm_surrogate *net, float max_residual_ms, int32_t n_probe,
+                                           pstm_learned_report *report, void *stream);
+
 /* Wait for all work queued on the context's stream.  Replaces
  * MigrationKernel.synchronize, pstm/kernels/base.py:315. */
 int32_t pstm_cuda_synchronize(void *ctx);

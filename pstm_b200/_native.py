@@ -80,6 +80,30 @@ class TuneResult(ctypes.Structure):
     ]
 
 
+class SurrogateDomain(ctypes.Structure):
+    _fields_ = [
+        ("traveltime", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("curved_v0", ctypes.c_double), ("curved_k", ctypes.c_double),
+        ("t0_max_s", ctypes.c_double), ("h_max_m", ctypes.c_double),
+        ("v_a", ctypes.c_double), ("v_b", ctypes.c_double), ("v_rel", ctypes.c_double),
+        ("eta_slope", ctypes.c_double), ("eta_jitter", ctypes.c_double), ("eta_max", ctypes.c_double),
+    ]
+
+
+class Surrogate(ctypes.Structure):
+    _fields_ = [
+        ("shift", ctypes.c_float * 8), ("scale", ctypes.c_float * 8), ("out_scale", ctypes.c_float),
+        ("traveltime", ctypes.c_int32), ("params", _vp),
+    ]
+
+
+class LearnedReport(ctypes.Structure):
+    _fields_ = [
+        ("probe_max_ms", ctypes.c_float), ("probe_rms_ms", ctypes.c_float),
+        ("n_probe_used", ctypes.c_int32), ("used_surrogate", ctypes.c_int32),
+    ]
+
+
 # name -> (restype, argtypes); the exported surface of include/pstm_cuda.h
 SIGNATURES = {
     "pstm_cuda_abi_version": (ctypes.c_int32, []),
@@ -98,6 +122,18 @@ SIGNATURES = {
                                                  ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params),
                                                  ctypes.POINTER(BinDesc), ctypes.c_int32, ctypes.c_int64,
                                                  ctypes.POINTER(TuneResult)]),
+    "pstm_cuda_surrogate_param_count": (ctypes.c_int32, []),
+    "pstm_cuda_surrogate_samples": (ctypes.c_int32, [_vp, ctypes.POINTER(SurrogateDomain), ctypes.c_uint64,
+                                                     ctypes.c_int64, ctypes.c_int32, _vp, _vp, _vp, _vp]),
+    "pstm_cuda_surrogate_gradients": (ctypes.c_int32, [_vp, ctypes.POINTER(Surrogate), _vp, _vp, ctypes.c_int32,
+                                                       _vp, _vp, _vp]),
+    "pstm_cuda_surrogate_adam": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int32, ctypes.c_float, _vp]),
+    "pstm_cuda_surrogate_eval": (ctypes.c_int32, [_vp, ctypes.POINTER(Surrogate), _vp, ctypes.c_int32, _vp, _vp]),
+    "pstm_cuda_migrate_tile_learned_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc),
+                                                            ctypes.POINTER(OutputDesc), ctypes.POINTER(VelocityDesc),
+                                                            ctypes.POINTER(Params), ctypes.POINTER(Surrogate),
+                                                            ctypes.c_float, ctypes.c_int32,
+                                                            ctypes.POINTER(LearnedReport), _vp]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
 }

@@ -278,6 +278,7 @@ void release_batch(Ctx *c) {
     release(c->counter);
     release(c->tune_image);
     release(c->tune_fold);
+    release(c->probe);
 }
 }  // namespace ctx
 }  // namespace pstm

@@ -79,8 +79,14 @@ int32_t validate(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out
     return rc ? fail(c, rc, msg) : PSTM_OK;
 }
 
-int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
-                const pstm_velocity_desc *vel, const pstm_params *prm, cudaStream_t st) {
+}  // namespace
+
+namespace pstm {
+namespace ctx {
+
+int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
+                     const pstm_params *prm, cudaStream_t st, TilePlan &tp) {
+    tp.empty = true;
     int32_t rc = validate(c, tr, out, vel, prm);
     if (rc) return rc;
     if (injected("migrate")) return fail(c, PSTM_ERR_INJECTED, "injected fault: migrate");
@@ -88,7 +94,8 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
     int R, PB;
     plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB);
-    KParams P = make_params(tr, out, vel, prm, PB);
+    KParams &P = tp.P;
+    P = make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // nothing to add: image += 0, fold += 0
 
     const bool per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
@@ -151,17 +158,42 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     const int tb = kThreads * R;
     const int nblk_t = (out->nt + tb - 1) / tb;
     if (nblk_p > 0x7fffffff || nblk_t > 65535) return fail(c, PSTM_ERR_UNSUPPORTED, "tile too large for one launch");
-    Launch L;
-    L.grid = dim3((unsigned)nblk_p, (unsigned)nblk_t);
-    L.smem = smem;
-    L.stream = st;
-    e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, exact, L);
-    if (e != cudaSuccess) return cuda_fail(c, e, "migrate kernel launch");
+    tp.Pg = Pg;
+    tp.L = Launch();
+    tp.L.grid = dim3((unsigned)nblk_p, (unsigned)nblk_t);
+    tp.L.smem = smem;
+    tp.L.stream = st;
+    tp.tt = prm->traveltime;
+    tp.amp = tr->amp_dtype;
+    tp.per_pillar = per_pillar;
+    tp.exact = exact;
+    tp.n_p = n_p;
+    tp.empty = false;
     return PSTM_OK;
 }
 
+int32_t launch_tile(Ctx *c, const TilePlan &tp) {
+    const cudaError_t e = launch_kind(tp.tt, tp.P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, tp.L);
+    return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "migrate kernel launch");
+}
+
+}  // namespace ctx
+}  // namespace pstm
+
+namespace {
+
+int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
+                const pstm_velocity_desc *vel, const pstm_params *prm, cudaStream_t st) {
+    TilePlan tp;
+    const int32_t rc = prepare_tile(c, tr, out, vel, prm, st, tp);
+    if (rc || tp.empty) return rc;
+    return launch_tile(c, tp);
+}
+
+}  // namespace
+
 // Read back the kernels' error word (after the stream has drained).
-int32_t check_error_word(Ctx *c) {
+int32_t pstm::ctx::check_error_word(Ctx *c) {
     if (!c->errword.ptr) return PSTM_OK;
     int32_t w = 0;
     cudaError_t e = cudaMemcpy(&w, c->errword.ptr, sizeof(w), cudaMemcpyDeviceToHost);
@@ -170,6 +202,8 @@ int32_t check_error_word(Ctx *c) {
         return fail(c, PSTM_ERR_TIMEOUT, "a bounded wait for a trace-row copy gave up; the tile was not written");
     return PSTM_OK;
 }
+
+namespace {
 
 template <typename T>
 cudaError_t stage(DevBuf &b, const T *src, size_t count, cudaStream_t st, const T **dst) {

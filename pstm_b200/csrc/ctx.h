@@ -8,6 +8,9 @@
 #include <string>
 #include <vector>
 
+#include "pstm_cuda.h"
+#include "launch.h"
+
 namespace pstm {
 namespace ctx {
 
@@ -34,10 +37,28 @@ struct Ctx {
     int smem_optin = 0;   // max dynamic shared memory per block
     // batched form
     DevBuf bins, counter, tune_image, tune_fold;
+    DevBuf probe;                           // learned form: per-probe residuals
     std::vector<unsigned char> graph_key;   // arguments the cached graph was captured with
     cudaGraphExec_t graph = nullptr;
     std::map<std::string, Shape> tuned;     // autotuned shapes by workload class
 };
+
+// A per-tile launch prepared by prepare_tile: tables, packed geometry and the
+// device parameter block are enqueued; the migration launch is not.
+struct TilePlan {
+    KParams P;
+    const KParams *Pg = nullptr;
+    Launch L;
+    int tt = 0, amp = 0;
+    bool per_pillar = false, exact = false;
+    int64_t n_p = 0;
+    bool empty = true;   // no traces: nothing to launch
+};
+
+int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
+                     const pstm_params *prm, cudaStream_t st, TilePlan &tp);
+int32_t launch_tile(Ctx *c, const TilePlan &tp);
+int32_t check_error_word(Ctx *c);   // after the stream has drained
 
 int32_t fail(Ctx *c, int32_t code, const std::string &msg);
 int32_t cuda_fail(Ctx *c, cudaError_t e, const char *what);

@@ -212,23 +212,19 @@ __device__ __forceinline__ float taper_weight(float x) {
 // ---------------------------------------------------------------- FP64 exact decisions
 // (rare paths: they read the launch parameters from a global copy, so the
 // kernel's own parameter block never has its address taken)
+// FP64 traveltime of one pair from its raw quantities: output time t0 (s),
+// squared horizontal source and receiver distances, v_rms, eta and the
+// curved-ray (v0, k).  The oracle's formulas; also the surrogate's target.
 template <int TT>
-__device__ double exact_traveltime(const KParams *P, int64_t tr, int p, int t, double ox, double oy) {
-    const double t0 = P->ta[t] / 1000.0;
-    const double v = P->vel3d ? P->vrms[(int64_t)p * P->nt + t] : P->vrms[t];
-    const double dxs = ox - P->sx[tr], dys = oy - P->sy[tr];
-    const double dxr = ox - P->rx[tr], dyr = oy - P->ry[tr];
-    const double ds2 = dxs * dxs + dys * dys, dr2 = dxr * dxr + dyr * dyr;
+__host__ __device__ inline double traveltime_fp64(double t0, double ds2, double dr2, double v, double eta, double v0,
+                                                  double k) {
     const double t0h = t0 * 0.5;
-    double eta = P->eta_const;
-    if (P->eta) eta = P->eta3d ? P->eta[(int64_t)p * P->nt + t] : P->eta[t];
     auto vti_corr = [&](double h2) {
         const double v2 = v * v;
         const double den = v2 * (t0h * t0h * v2 + (1.0 + 2.0 * eta) * h2);
         return fabs(den) > 1e-20 ? (2.0 * eta * h2 * h2) / den : 0.0;
     };
     auto curved_leg = [&](double h2) {
-        const double k = P->cr_k, v0 = P->cr_v0;
         if (fabs(k) < 1e-10) {
             const double z = v0 * t0h;
             const double r = sqrt(h2 + z * z);
@@ -261,6 +257,17 @@ __device__ double exact_traveltime(const KParams *P, int64_t tr, int p, int t, d
         };
         return leg(ds2) + leg(dr2);
     }
+}
+
+template <int TT>
+__device__ double exact_traveltime(const KParams *P, int64_t tr, int p, int t, double ox, double oy) {
+    const double t0 = P->ta[t] / 1000.0;
+    const double v = P->vel3d ? P->vrms[(int64_t)p * P->nt + t] : P->vrms[t];
+    const double dxs = ox - P->sx[tr], dys = oy - P->sy[tr];
+    const double dxr = ox - P->rx[tr], dyr = oy - P->ry[tr];
+    double eta = P->eta_const;
+    if (P->eta) eta = P->eta3d ? P->eta[(int64_t)p * P->nt + t] : P->eta[t];
+    return traveltime_fp64<TT>(t0, dxs * dxs + dys * dys, dxr * dxr + dyr * dyr, v, eta, P->cr_v0, P->cr_k);
 }
 
 // Is the FP64 sample index of this pair inside [0, ns-1)?

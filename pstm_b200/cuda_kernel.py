@@ -124,6 +124,56 @@ class CudaKernel:
     def migrate_tile_curved_vti(self, traces, output, velocity, config=None) -> KernelMetrics:
         return self._migrate(traces, output, velocity, config, nat.TT_CURVED_VTI)
 
+    def migrate_tile_learned(self, traces, output, velocity, surrogate, config=None,
+                             kernel_type: str = "anisotropic_vti", max_residual_ms: float = 0.1,
+                             n_probe: int = 4096):
+        """The learned form: probe ``surrogate`` (a ``pstm_b200.surrogate.Net``)
+        against the exact traveltime on ``n_probe`` random in-aperture pairs of
+        this tile and migrate with it when the largest residual is at most
+        ``max_residual_ms`` (negative: always), else with the exact kernel.
+        Device tensors only.  Returns (KernelMetrics, report dict)."""
+        if self._ctx is None or self._config is None:
+            raise RuntimeError("Kernel not initialized")
+        if kernel_type not in ("anisotropic_vti", "curved_vti"):
+            raise ValueError("the learned form covers anisotropic_vti and curved_vti")
+        cfg = config if config is not None else self._config
+        t_start = time.perf_counter()
+        keep: list = []
+        devs: list = []
+        td = self._trace_desc(traces, keep, devs)
+        od = nat.OutputDesc()
+        img = output.image
+        if not _is_torch_cuda(img):
+            raise ValueError("the learned form takes CUDA tensors")
+        import torch
+        if img.dtype not in (torch.float64, torch.float32) or not img.is_contiguous():
+            raise ValueError("device image must be a contiguous float64/float32 tensor")
+        od.image = img.data_ptr()
+        od.image_dtype = nat.IMAGE_F64 if img.dtype == torch.float64 else nat.IMAGE_F32
+        if output.fold is not None:
+            od.fold = output.fold.data_ptr()
+            od.fold_is_3d = 1 if len(output.fold.shape) == 3 else 0
+            devs.append(_is_torch_cuda(output.fold))
+        self._output_axes(output, od, keep, devs)
+        vd = nat.VelocityDesc()
+        vd.vrms, vd.is_3d, dv = self._velocity(velocity, output, od.nx, od.ny, od.nt, keep)
+        devs.append(dv)
+        prm = self._params(cfg, _TT_BY_TYPE[kernel_type], keep, devs=devs)
+        if not all(devs):
+            raise ValueError("the learned form takes CUDA tensors only")
+        net = surrogate.to_struct()
+        rep = nat.LearnedReport()
+        stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+        rc = self._lib.pstm_cuda_migrate_tile_learned_dev(self._ctx, ctypes.byref(td), ctypes.byref(od),
+                                                          ctypes.byref(vd), ctypes.byref(prm), ctypes.byref(net),
+                                                          float(max_residual_ms), int(n_probe), ctypes.byref(rep),
+                                                          ctypes.c_void_p(stream))
+        nat.check(rc, self._ctx, self._lib)
+        report = {"probe_max_ms": rep.probe_max_ms, "probe_rms_ms": rep.probe_rms_ms,
+                  "n_probe_used": rep.n_probe_used, "used_surrogate": bool(rep.used_surrogate)}
+        return KernelMetrics(n_traces_processed=td.n_traces, n_samples_output=od.nx * od.ny * od.nt,
+                             compute_time_s=time.perf_counter() - t_start), report
+
     def migrate_bins(self, traces, bins, geometry, velocity, config=None,
                      kernel_type: str = "straight_ray") -> KernelMetrics:
         """The batched form; see :func:`migrate_bins`."""

@@ -58,6 +58,11 @@ def test_null_context_errors_without_gpu(lib_path):
     assert rc == nat.ERR_NOT_INITIALIZED
     assert L.pstm_cuda_migrate_bins_dev(None, None, None, None, None, None, 0, None) == nat.ERR_NOT_INITIALIZED
     assert L.pstm_cuda_autotune_bins(None, None, None, None, None, None, 0, 0, None) == nat.ERR_NOT_INITIALIZED
+    assert L.pstm_cuda_surrogate_param_count() == 8897
+    assert L.pstm_cuda_surrogate_samples(None, None, 0, 0, 0, None, None, None, None) == nat.ERR_NOT_INITIALIZED
+    assert L.pstm_cuda_surrogate_eval(None, None, None, 0, None, None) == nat.ERR_NOT_INITIALIZED
+    assert L.pstm_cuda_migrate_tile_learned_dev(None, None, None, None, None, None, 0.0, 0, None,
+                                                None) == nat.ERR_NOT_INITIALIZED
     with pytest.raises(RuntimeError, match="not initialized"):
         nat.check(rc, None, L)
 
@@ -68,7 +73,9 @@ def _c_layout(tmp_path):
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pstm_cuda.h"', 'int main(void){']
     for cname, cls in (("pstm_traces_desc", nat.TracesDesc), ("pstm_output_desc", nat.OutputDesc),
                        ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params),
-                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult)):
+                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult),
+                       ("pstm_surrogate_domain", nat.SurrogateDomain), ("pstm_surrogate", nat.Surrogate),
+                       ("pstm_learned_report", nat.LearnedReport)):
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for f, _ in cls._fields_:
             lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
@@ -86,7 +93,9 @@ def test_ctypes_structs_match_header_layout(tmp_path):
     lay = _c_layout(tmp_path)
     for cname, cls in (("pstm_traces_desc", nat.TracesDesc), ("pstm_output_desc", nat.OutputDesc),
                        ("pstm_velocity_desc", nat.VelocityDesc), ("pstm_params", nat.Params),
-                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult)):
+                       ("pstm_bin_desc", nat.BinDesc), ("pstm_tune_result", nat.TuneResult),
+                       ("pstm_surrogate_domain", nat.SurrogateDomain), ("pstm_surrogate", nat.Surrogate),
+                       ("pstm_learned_report", nat.LearnedReport)):
         assert lay[(cname, "size")] == ctypes.sizeof(cls), cname
         for f, _ in cls._fields_:
             assert lay[(cname, f)] == getattr(cls, f).offset, (cname, f)
