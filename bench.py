@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision-form measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-form measurement")
+    ap.add_argument("--learned-steps", type=int, default=60000, help="Adam steps of the surrogate training")
     ap.add_argument("--batch-scale", type=int, default=16,
                     help="the batched form migrates 1/this of every bin's traces (1: the full ~2M traces)")
     return ap.parse_args()
@@ -367,6 +369,87 @@ def measure_batched(args, world, dist):
     }
 
 
+def measure_learned(args, sv, amps, world, dist):
+    """The learned form on the curved/VTI case (case-2 geometry and velocity,
+    eta(t0) = 0.15 t0 / 3 s): train the surrogate with the package's own
+    kernels on seeded exact targets, report its traveltime error in ms on
+    held-out samples, then migrate a sample tile (24 x 24 pillars x 1500
+    samples x 65,536 traces, FP32 traces) three ways: exact VTI kernel, the
+    learned entry point with the 0.1 ms probe (which falls back to the exact
+    kernel when the probe fails) and the surrogate forced on every pair."""
+    import dataclasses
+    import torch
+    from pstm_b200 import replicas, workloads
+    from pstm_b200 import surrogate as S
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    tr = S.Trainer(int(os.environ.get("LOCAL_RANK", "0")))
+    dom = S.survey_domain("anisotropic_vti", t0_max_s=(NT - 1) * DT_MS / 1000.0, h_max_m=GRID * DX)
+    t0 = time.perf_counter()
+    net = tr.train(dom, n_train=50_000_000, steps=args.learned_steps, batch=65536, lr=2e-3,
+                   log_every=max(1, args.learned_steps // 4))
+    train_s = time.perf_counter() - t0
+    err = tr.error_ms(net, n=1 << 20)
+    tr.close()
+
+    n_tr, P = 1 << 16, 24
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    tb = TraceBlock(amplitudes=amps[:n_tr].float().contiguous(), source_x=dev(sv.s[:n_tr, 0]),
+                    source_y=dev(sv.s[:n_tr, 1]), receiver_x=dev(sv.r[:n_tr, 0]), receiver_y=dev(sv.r[:n_tr, 1]),
+                    offset=dev(np.hypot(*(sv.r[:n_tr] - sv.s[:n_tr]).T)),
+                    midpoint_x=dev((sv.s[:n_tr, 0] + sv.r[:n_tr, 0]) / 2), midpoint_y=dev((sv.s[:n_tr, 1] + sv.r[:n_tr, 1]) / 2),
+                    sample_rate_ms=DT_MS, start_time_ms=0.0)
+    ix0 = iy0 = 120
+    out, vel = sv.tile(ix0, ix0 + P, iy0, iy0 + P)
+    eta = workloads.survey_eta(sv.t_axis_ms)
+    cfg = workloads.survey_config(kernel_type="anisotropic_vti", aa=True, dx=DX, eta=eta)
+    cfg.vti_eta_array = dev(eta)
+    dvel = VelocitySlice(vrms=dev(vel.vrms), is_1d=False)
+
+    def fresh():
+        return OutputTile(image=torch.zeros(out.image.shape, dtype=torch.float64, device="cuda"),
+                          fold=torch.zeros(out.fold.shape, dtype=torch.int32, device="cuda"),
+                          x_axis=dev(out.x_axis), y_axis=dev(out.y_axis), t_axis_ms=dev(out.t_axis_ms))
+    k = CudaKernel(precision="fast")
+    k.initialize(cfg)
+    pairs = P * P * NT * n_tr
+
+    def timed(fn):
+        o = fresh()
+        fn(o)
+        torch.cuda.synchronize()
+        o = fresh()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn(o)
+        e1.record()
+        torch.cuda.synchronize()
+        return replicas.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda"), o, r
+
+    ms_exact, o_exact, _ = timed(lambda o: k.migrate_tile_vti(tb, o, dvel, cfg))
+    ms_probe, o_probe, r_probe = timed(lambda o: k.migrate_tile_learned(tb, o, dvel, net, cfg, max_residual_ms=0.1)[1])
+    ms_forced, o_forced, r_forced = timed(lambda o: k.migrate_tile_learned(tb, o, dvel, net, cfg,
+                                                                           max_residual_ms=-1.0)[1])
+    k.cleanup()
+    ref = o_exact.image.cpu().numpy()
+    rel = lambda a: float(np.linalg.norm(a.image.cpu().numpy() - ref) / np.linalg.norm(ref))
+    return {
+        "value": world * pairs / (ms_probe / 1e3), "unit": UNIT,
+        "traveltime": "anisotropic_vti", "trace_dtype": "f32",
+        "sample": f"{P}x{P} pillars x {NT} samples x {n_tr} traces of the case-2 tile (eta(t0) = 0.15 t0/3 s)",
+        "exact_value": world * pairs / (ms_exact / 1e3),
+        "learned_with_probe": {"value": world * pairs / (ms_probe / 1e3), **r_probe,
+                               "rel_l2_vs_exact_kernel": rel(o_probe)},
+        "learned_forced": {"value": world * pairs / (ms_forced / 1e3), **r_forced,
+                           "rel_l2_vs_exact_kernel": rel(o_forced)},
+        "surrogate": {"layers": "7-64-64-64-1 SiLU, BF16 weights, FP32 accumulate (mma.sync m16n8k16)",
+                      "target": "T_exact - T_DSR(v_rms), exact FP64 targets", "train_samples": 50_000_000,
+                      "steps": args.learned_steps, "batch": 65536, "train_seconds": train_s,
+                      "loss_history": net.history, "heldout_error": err},
+        "threshold_ms": 0.1,
+    }
+
+
 # ------------------------------------------------------------------ our arm
 def main_ours(args):
     import torch
@@ -507,6 +590,9 @@ def main_ours(args):
     if not args.no_batched:
         forms = forms or {}
         forms["batched_offset_bins_bf16_vti"] = measure_batched(args, world, dist)
+    if not args.no_learned:
+        forms = forms or {}
+        forms["learned_vti"] = measure_learned(args, sv, amps, world, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
