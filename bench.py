@@ -46,9 +46,9 @@ FLOP_PER_PAIR = 20
 MUFU_PER_PAIR = 4
 
 # DRAM traffic of one 64 x 64 x 1500 tile launch per trace of the panel, from an
-# ncu capture (dram__bytes) of the same launch at 32,768 traces: 14.45 GB; the
-# traffic grows in proportion to the traces streamed (profiles/migrate_kernel_case2.md)
-DRAM_BYTES_PER_TRACE_TILE64 = 14.45e9 / 32768
+# ncu capture (dram__bytes) of the same launch at 32,768 traces: 5.04 GB; the
+# traffic grows in proportion to the traces streamed
+DRAM_BYTES_PER_TRACE_TILE64 = 5.04e9 / 32768
 
 
 def parse():
