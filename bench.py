@@ -68,6 +68,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-form measurement")
     ap.add_argument("--learned-steps", type=int, default=60000, help="Adam steps of the surrogate training")
+    ap.add_argument("--case5", action="store_true",
+                    help="run the large-survey case (512x512x2000, FP16 traces, curved+VTI) instead")
+    ap.add_argument("--case5-tiles", type=int, default=2, help="64x64 tiles of the case-5 grid to migrate")
+    ap.add_argument("--case5-aperture", type=float, default=1000.0, help="max aperture (m) of the case-5 run")
     ap.add_argument("--batch-scale", type=int, default=16,
                     help="the batched form migrates 1/this of every bin's traces (1: the full ~2M traces)")
     return ap.parse_args()
@@ -628,8 +632,135 @@ def main_ours(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ case 5
+def main_case5(args):
+    """The large-survey case: 512 x 512 bins at 12.5 m x 2000 samples at 2 ms
+    (2.1 GB FP32 image), 8,388,608 FP16 traces of 2000 samples (33.6 GB, all
+    resident in HBM) with offsets up to 5 km over a 6.4 km patch, curved-ray +
+    VTI traveltime (learned surrogate with the exact fallback), triangle AA and
+    weights on.  The tiled executor migrates --case5-tiles 64 x 64 tiles; the
+    aperture is capped at --case5-aperture m so that the FP64 oracle check of
+    64 random output traces stays feasible.  Prints one JSON line."""
+    import torch
+    from oracle import oracle
+    from pstm_b200 import build, replicas, workloads
+    from pstm_b200 import surrogate as S
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    from pstm_b200.executor import TiledExecutor, tile_ranges
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    build.build()
+    G5, NT5, NS5, N5 = 512, 2000, 2000, args.traces if args.traces != (1 << 20) else 8_388_608
+    t_gen = time.perf_counter()
+    sv, amps = workloads.survey_device(N5, G5, G5, NT5, DT_MS, NS5, dx=DX, max_offset=5000.0, seed=55,
+                                       dtype=torch.float16)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    mx, my = (sv.s[:, 0] + sv.r[:, 0]) / 2.0, (sv.s[:, 1] + sv.r[:, 1]) / 2.0
+    tb = TraceBlock(amplitudes=amps, source_x=dev(sv.s[:, 0]), source_y=dev(sv.s[:, 1]), receiver_x=dev(sv.r[:, 0]),
+                    receiver_y=dev(sv.r[:, 1]), offset=dev(np.hypot(*(sv.r - sv.s).T)), midpoint_x=dev(mx),
+                    midpoint_y=dev(my), sample_rate_ms=DT_MS, start_time_ms=0.0)
+    vfull = dev(sv.velocity())
+    gen_s = time.perf_counter() - t_gen
+    eta = workloads.survey_eta(sv.t_axis_ms)
+    cfg = workloads.survey_config(kernel_type="curved_vti", aa=True, dx=DX, eta=eta, v0=1500.0, k=0.5)
+    cfg.max_aperture_m = args.case5_aperture
+    cfg.vti_eta_array = dev(eta)
+    tr = S.Trainer(int(os.environ.get("LOCAL_RANK", "0")))
+    t0 = time.perf_counter()
+    dom = S.survey_domain("curved_vti", t0_max_s=(NT5 - 1) * DT_MS / 1000.0,
+                          h_max_m=64 * DX + args.case5_aperture + 2500.0, v0=1500.0, k=0.5)
+    net = tr.train(dom, n_train=50_000_000, steps=args.learned_steps, batch=65536, lr=2e-3,
+                   log_every=max(1, args.learned_steps // 4))
+    train_s = time.perf_counter() - t0
+    heldout = tr.error_ms(net, n=1 << 20)
+    tr.close()
+
+    k = CudaKernel(precision="fast")
+    k.initialize(cfg)
+    ex = TiledExecutor(k, tb, sv.x_axis, sv.y_axis, sv.t_axis_ms,
+                       lambda x0, x1, y0, y1: VelocitySlice(vrms=vfull[x0:x1, y0:y1].contiguous(), is_1d=False),
+                       cfg, kernel_type="curved_vti", tile=64, surrogate=net, max_residual_ms=0.1)
+    tiles_all = tile_ranges(G5, G5, 64)
+    centre = sorted(tiles_all, key=lambda t: abs(t[0] + 32 - G5 / 2) + abs(t[2] + 32 - G5 / 2))
+    tiles = centre[:max(1, args.case5_tiles)]
+    image = torch.zeros((G5, G5, NT5), dtype=torch.float32, device="cuda")
+    fold = torch.zeros((G5, G5), dtype=torch.int32, device="cuda")
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        results = ex.run(image, fold, tiles)
+    clocks = clk.summary()
+    pairs = sum(r.pairs for r in results)
+    kernel_s = sum(r.kernel_ms for r in results) / 1e3
+    value = pairs / kernel_s
+
+    # FP64 oracle on 64 random output traces of the first tile, each against a
+    # seeded 1/32 sample of that tile's selected traces (the same sample on the GPU)
+    rng = np.random.default_rng(5)
+    ix0, ix1, iy0, iy1 = tiles[0]
+    pix = rng.integers(ix0, ix1, 64)
+    piy = rng.integers(iy0, iy1, 64)
+    idx = ex.select(tiles[0])[::32]
+    sub = ex._gather(idx)
+    xg, yg = sv.x_axis[pix].reshape(64, 1), sv.y_axis[piy].reshape(64, 1)
+    v64 = vfull[dev(pix), dev(piy)].cpu().numpy().reshape(64, 1, NT5)
+    g_out = OutputTile(image=torch.zeros((64, 1, NT5), dtype=torch.float64, device="cuda"),
+                       fold=torch.zeros((64, 1), dtype=torch.int32, device="cuda"),
+                       x_axis=dev(np.arange(64.0)), y_axis=dev(np.zeros(1)), t_axis_ms=dev(sv.t_axis_ms),
+                       x_grid=dev(xg), y_grid=dev(yg))
+    _, rep = k.migrate_tile_learned(sub, g_out, VelocitySlice(vrms=dev(v64), is_1d=False), net, cfg,
+                                    kernel_type="curved_vti", max_residual_ms=0.1)
+    torch.cuda.synchronize()
+    k.cleanup()
+    from pstm_b200.base import create_trace_block
+    ii = idx.cpu().numpy()
+    htb = create_trace_block(sub.amplitudes.float().cpu().numpy(), sv.s[ii, 0], sv.s[ii, 1], sv.r[ii, 0],
+                             sv.r[ii, 1], sample_rate_ms=DT_MS)
+    o_out = OutputTile(image=np.zeros((64, 1, NT5)), fold=np.zeros((64, 1), np.int32), x_axis=np.arange(64.0),
+                       y_axis=np.zeros(1), t_axis_ms=sv.t_axis_ms, x_grid=xg, y_grid=yg)
+    ocfg = workloads.survey_config(kernel_type="curved_vti", aa=True, dx=DX, eta=eta, v0=1500.0, k=0.5)
+    ocfg.max_aperture_m = args.case5_aperture
+    t_or = time.perf_counter()
+    oracle.build()
+    oracle.migrate(htb, o_out, VelocitySlice(vrms=v64, is_1d=False), ocfg, kind="curved_vti")
+    oracle_s = time.perf_counter() - t_or
+    got = g_out.image.cpu().numpy()
+    err = float(np.linalg.norm(got - o_out.image) / np.linalg.norm(o_out.image))
+    fold_ok = bool((g_out.fold.cpu().numpy() == o_out.fold).all())
+
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    mufu_peak = 148 * 16 * sm_mhz * 1e6
+    mufu_per_pair = 8   # straight DSR 3 + AA 1 + curved legs 2 + VTI 2
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": len(results), "warmup": 0,
+        "ms_per_step": 1e3 * kernel_s / len(results), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+        "config": {"workload": "case-5 large survey: 512x512 bins @12.5 m x 2000 samples @2 ms, 8,388,608 FP16 "
+                               "traces x 2000 (offsets <= 5 km, 6.4 km patch), curved-ray + VTI, AA + weights, "
+                               "tiled executor (one step = one 64x64 tile against its selected traces)",
+                   "traces": N5, "traces_resident_gb": N5 * NS5 * 2 / 1e9, "tiles_run": [list(t) for t in tiles],
+                   "max_aperture_m": args.case5_aperture, "image": "FP32 (512, 512, 2000) on the device"},
+        "tiles": [{"tile": list(r.tile), "selected_traces": r.n_traces, "pairs": r.pairs, "ms": r.kernel_ms,
+                   "used_surrogate": r.used_surrogate, "probe_max_ms": r.probe_max_ms} for r in results],
+        "roofline": {"bound": "sfu", "unit": "Gop/s", "achieved": value * mufu_per_pair / 1e9,
+                     "peak": mufu_peak / 1e9, "frac": value * mufu_per_pair / mufu_peak,
+                     "per_pair": f"{mufu_per_pair} MUFU (DSR 3 + AA 1 + curved 2 + VTI 2)",
+                     "peak_source": "derived: 148 SMs x 16 MUFU/clk x median SM clock"},
+        "oracle_check": {"rel_l2_vs_fp64": err, "fold_bit_exact": fold_ok, "pillars": 64,
+                         "sample": f"64 random output traces of tile {list(tiles[0])} x {NT5} samples against "
+                                   f"every 32nd of its {int(ex.select(tiles[0]).numel())} selected traces "
+                                   f"({int(idx.numel())} traces)", "oracle_seconds": oracle_s,
+                         "used_surrogate": rep["used_surrogate"]},
+        "surrogate": {"train_seconds": train_s, "steps": args.learned_steps, "heldout_error": heldout},
+        "generation_seconds": gen_s, "wall_seconds_tiles": ex.wall_s, "clocks": clocks,
+        "gpu_launches": 3 * len(results),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.case5:
+        main_case5(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     else:
