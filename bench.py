@@ -261,6 +261,44 @@ def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, 
     return res
 
 
+def measure_case1():
+    """The CPU-runnable case: 64 x 64 bins at 25 m x 500 samples at 4 ms against
+    16,384 FP32 traces of 500 samples (3.36e10 pairs), straight rays, aperture
+    1000 m, weights on, AA off; device-resident inputs, CUDA events."""
+    import torch
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    case = workloads.config1()
+    tb, out = case.traces, case.output
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    dtb = TraceBlock(amplitudes=dev(tb.amplitudes), source_x=dev(tb.source_x), source_y=dev(tb.source_y),
+                     receiver_x=dev(tb.receiver_x), receiver_y=dev(tb.receiver_y), offset=dev(tb.offset),
+                     midpoint_x=dev(tb.midpoint_x), midpoint_y=dev(tb.midpoint_y),
+                     sample_rate_ms=tb.sample_rate_ms, start_time_ms=tb.start_time_ms)
+    o = OutputTile(image=torch.zeros(out.image.shape, dtype=torch.float64, device="cuda"),
+                   fold=torch.zeros(out.fold.shape, dtype=torch.int32, device="cuda"),
+                   x_axis=dev(out.x_axis), y_axis=dev(out.y_axis), t_axis_ms=dev(out.t_axis_ms))
+    vel = VelocitySlice(vrms=dev(case.velocity.vrms), is_1d=True)
+    k = CudaKernel()
+    k.initialize(case.config)
+    for _ in range(3):
+        k.migrate_tile(dtb, o, vel)
+    torch.cuda.synchronize()
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        k.migrate_tile(dtb, o, vel)
+    e1.record()
+    torch.cuda.synchronize()
+    k.cleanup()
+    ms = e0.elapsed_time(e1) / reps
+    return {"value": case.pairs / (ms / 1e3), "unit": UNIT, "ms_per_tile": ms, "pairs": case.pairs,
+            "workload": "case 1: 64x64x500 tile, 16,384 FP32 traces x 500 @4 ms, straight exact, AA off",
+            "l2": "inputs (33 MB) fit in L2; consecutive calls on the same tile"}
+
+
 def measure_batched(args, world, dist):
     """The batched form on the common-offset case: 40 offset bins over 0-4 km,
     lognormal trace counts between 5k and 200k (about 2M), 1000 BF16 samples at
@@ -589,12 +627,15 @@ def main_ours(args):
         ke.cleanup()
 
     forms = None
-    if not args.no_forms:
+    # the forms are single-GPU measurements: every rank skips them alike when N > 1
+    single = world == 1
+    if not args.no_forms and single:
         forms = measure_forms(args, k, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg)
-    if not args.no_batched:
+        forms["case1_tile"] = measure_case1()
+    if not args.no_batched and single:
         forms = forms or {}
         forms["batched_offset_bins_bf16_vti"] = measure_batched(args, world, dist)
-    if not args.no_learned:
+    if not args.no_learned and single:
         forms = forms or {}
         forms["learned_vti"] = measure_learned(args, sv, amps, world, dist)
 

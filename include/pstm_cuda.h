@@ -288,6 +288,15 @@ int32_t pstm_cuda_migrate_tile_learned_dev(void *ctx, const pstm_traces_desc *tr
                                            const pstm_surrogate *net, float max_residual_ms, int32_t n_probe,
                                            pstm_learned_report *report, void *stream);
 
+/* Linear interpolation of n_rows rows of n_src samples (dtype: PSTM_IMAGE_F64
+ * or PSTM_IMAGE_F32) from the ascending times src_times onto dst_times, the
+ * edge value outside (np.interp's rule); all device pointers.  Replaces the
+ * per-trace np.interp of resample_to_uniform,
+ * pstm/algorithm/time_variant.py:354-397, for device images. */
+int32_t pstm_cuda_interp_rows(void *ctx, int32_t dtype, const void *src, int64_t n_rows, int32_t n_src,
+                              const double *src_times, int32_t n_dst, const double *dst_times, void *dst,
+                              void *stream);
+
 /* Wait for all work queued on the context's stream.  Replaces
  * MigrationKernel.synchronize, pstm/kernels/base.py:315. */
 int32_t pstm_cuda_synchronize(void *ctx);

@@ -134,6 +134,8 @@ SIGNATURES = {
                                                             ctypes.POINTER(Params), ctypes.POINTER(Surrogate),
                                                             ctypes.c_float, ctypes.c_int32,
                                                             ctypes.POINTER(LearnedReport), _vp]),
+    "pstm_cuda_interp_rows": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, ctypes.c_int32, _vp,
+                                               ctypes.c_int32, _vp, _vp, _vp]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
 }

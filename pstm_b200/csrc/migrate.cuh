@@ -47,6 +47,16 @@ constexpr int kMaxChunk = 32;        // traces per chunk, upper bound
 constexpr int kGeoDoubles = 8;       // packed geometry per trace: sx sy rx ry mx my w 0
 constexpr int kWaitIters = 1 << 20;  // bound of every mbarrier wait loop
 
+// Unroll factors of the pair loops (records without / with a lane in the taper band).
+#ifndef PSTM_UNROLL_PLAIN
+#define PSTM_UNROLL_PLAIN 4
+#endif
+#ifndef PSTM_UNROLL_TAPER
+#define PSTM_UNROLL_TAPER 2
+#endif
+#define PSTM_PRAGMA_STR(x) #x
+#define PSTM_UNROLL(n) _Pragma(PSTM_PRAGMA_STR(unroll n))
+
 // ---------------------------------------------------------------- math helpers
 __device__ __forceinline__ float sqrt_approx(float x) {
     float y;
@@ -676,12 +686,12 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 using Tr = std::true_type;
                 float a = 0.f;
                 if (!hard_cut) {
-#pragma unroll 4
+                    PSTM_UNROLL(PSTM_UNROLL_PLAIN)
                     for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{});
-#pragma unroll 2
+                    PSTM_UNROLL(PSTM_UNROLL_TAPER)
                     for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{});
                 } else {   // no taper: the aperture edge is a hard cut, ties are decided in FP64
-#pragma unroll 2
+                    PSTM_UNROLL(PSTM_UNROLL_TAPER)
                     for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{});
                 }
                 if constexpr (!EXACT) {   // second pass over the flagged records only

@@ -4,8 +4,10 @@ Drop-in for the reference's kernel backends (``pstm/kernels/base.py:290-318``):
 ``name``, ``capabilities``, ``initialize``, ``migrate_tile``, ``synchronize``,
 ``cleanup``, plus the optional methods the reference executor discovers with
 ``hasattr`` (``pstm/pipeline/executor.py:1710-1745``):
-``migrate_tile_curved_ray`` and ``migrate_tile_vti``.  ``migrate_tile_curved_vti``
-is an extension with no reference counterpart.
+``migrate_tile_curved_ray``, ``migrate_tile_vti`` and ``migrate_tile_time_variant``
+(:1712-1717).  ``migrate_tile_curved_vti``, ``migrate_tile_learned``,
+``migrate_bins`` and ``autotune_bins`` are extensions with no reference
+counterpart.
 
 Arguments are duck-typed, so the reference's own ``TraceBlock``/``OutputTile``/
 ``VelocitySlice``/``KernelConfig`` objects work as well as this package's
@@ -123,6 +125,60 @@ class CudaKernel:
 
     def migrate_tile_curved_vti(self, traces, output, velocity, config=None) -> KernelMetrics:
         return self._migrate(traces, output, velocity, config, nat.TT_CURVED_VTI)
+
+    def migrate_tile_time_variant(self, traces, output, velocity, config, windows) -> KernelMetrics:
+        """Migrate at the sample times of the time-variant ``windows`` (straight
+        rays; the reference's ``migrate_tile_time_variant``,
+        ``metal_compiled.py:940-1275``).  As the reference, ``output.image`` is
+        replaced by the (nx, ny, n_windowed_samples) image, which the caller
+        brings back to the uniform axis with ``time_variant.resample_to_uniform``;
+        the fold (per pillar, the same at every time) is added into
+        ``output.fold``.  Host arrays or CUDA tensors, like ``migrate_tile``."""
+        from . import time_variant as tvm
+        from .base import OutputTile, VelocitySlice
+        if self._ctx is None or self._config is None:
+            raise RuntimeError("Kernel not initialized")
+        cfg = config if config is not None else self._config
+        t_start = time.perf_counter()
+        tv = tvm.window_times(windows)
+        if len(tv) == 0:
+            raise ValueError("no time windows")
+        nx, ny = len(output.x_axis), len(output.y_axis)
+        on_dev = _is_torch_cuda(output.image)
+        t_out = output.t_axis_ms.cpu().numpy() if _is_torch_cuda(output.t_axis_ms) else np.asarray(output.t_axis_ms)
+        v = velocity.vrms
+        vt = getattr(velocity, "t_axis_ms", None)
+        vt = t_out if vt is None else (vt.cpu().numpy() if _is_torch_cuda(vt) else np.asarray(vt, np.float64))
+        is_1d = bool(getattr(velocity, "is_1d", True))
+        if is_1d:
+            v_np = v.cpu().numpy() if _is_torch_cuda(v) else np.asarray(v, np.float64)
+            v_tv = np.interp(tv, vt[:len(v_np)], v_np)
+            if on_dev:
+                import torch
+                v_tv = torch.as_tensor(v_tv, device=output.image.device)
+        else:
+            v_tv = tvm.interp_rows(v, vt[:v.shape[-1]], tv, ctx=self._ctx if _is_torch_cuda(v) else None)
+        if on_dev:
+            import torch
+            dev = output.image.device
+            img = torch.zeros((nx, ny, len(tv)), dtype=output.image.dtype, device=dev)
+            fold = torch.zeros((nx, ny), dtype=torch.int32, device=dev)
+            t_axis = torch.as_tensor(tv, device=dev)
+        else:
+            img = np.zeros((nx, ny, len(tv)), dtype=np.asarray(output.image).dtype)
+            fold = np.zeros((nx, ny), np.int32)
+            t_axis = tv
+        tv_out = OutputTile(image=img, fold=fold, x_axis=output.x_axis, y_axis=output.y_axis, t_axis_ms=t_axis,
+                            x_grid=getattr(output, "x_grid", None), y_grid=getattr(output, "y_grid", None))
+        self._migrate(traces, tv_out, VelocitySlice(vrms=v_tv, is_1d=is_1d), cfg, nat.TT_STRAIGHT)
+        output.image = img
+        if output.fold is not None:
+            if len(output.fold.shape) == 3:
+                output.fold += fold[..., None]
+            else:
+                output.fold += fold
+        return KernelMetrics(n_traces_processed=int(traces.amplitudes.shape[0]), n_samples_output=nx * ny * len(tv),
+                             compute_time_s=time.perf_counter() - t_start)
 
     def migrate_tile_learned(self, traces, output, velocity, surrogate, config=None,
                              kernel_type: str = "anisotropic_vti", max_residual_ms: float = 0.1,
