@@ -261,6 +261,41 @@ def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, 
     return res
 
 
+def measure_case1_interp(method: str = "sinc8"):
+    """The case-1 tile with a higher-order trace interpolator (the FP64
+    interpolation kernel) instead of linear: pairs/s on device inputs."""
+    import dataclasses
+    import torch
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    case = workloads.config1()
+    tb, out = case.traces, case.output
+    cfg = dataclasses.replace(case.config, interpolation_method=method)
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    dtb = TraceBlock(amplitudes=dev(tb.amplitudes), source_x=dev(tb.source_x), source_y=dev(tb.source_y),
+                     receiver_x=dev(tb.receiver_x), receiver_y=dev(tb.receiver_y), offset=dev(tb.offset),
+                     midpoint_x=dev(tb.midpoint_x), midpoint_y=dev(tb.midpoint_y),
+                     sample_rate_ms=tb.sample_rate_ms, start_time_ms=tb.start_time_ms)
+    o = OutputTile(image=torch.zeros(out.image.shape, dtype=torch.float64, device="cuda"),
+                   fold=torch.zeros(out.fold.shape, dtype=torch.int32, device="cuda"),
+                   x_axis=dev(out.x_axis), y_axis=dev(out.y_axis), t_axis_ms=dev(out.t_axis_ms))
+    vel = VelocitySlice(vrms=dev(case.velocity.vrms), is_1d=True)
+    k = CudaKernel()
+    k.initialize(cfg)
+    k.migrate_tile(dtb, o, vel, cfg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    k.migrate_tile(dtb, o, vel, cfg)
+    e1.record()
+    torch.cuda.synchronize()
+    k.cleanup()
+    ms = e0.elapsed_time(e1)
+    return {"value": case.pairs / (ms / 1e3), "unit": UNIT, "ms_per_tile": ms, "interpolation": method,
+            "workload": "case 1 tile with the FP64 higher-order interpolation kernel"}
+
+
 def measure_case1():
     """The CPU-runnable case: 64 x 64 bins at 25 m x 500 samples at 4 ms against
     16,384 FP32 traces of 500 samples (3.36e10 pairs), straight rays, aperture
@@ -632,6 +667,7 @@ def main_ours(args):
     if not args.no_forms and single:
         forms = measure_forms(args, k, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg)
         forms["case1_tile"] = measure_case1()
+        forms["case1_tile_sinc8"] = measure_case1_interp("sinc8")
     if not args.no_batched and single:
         forms = forms or {}
         forms["batched_offset_bins_bf16_vti"] = measure_batched(args, world, dist)

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define PSTM_CUDA_ABI_VERSION 2
+#define PSTM_CUDA_ABI_VERSION 3
 
 typedef enum {
     PSTM_OK = 0,
@@ -49,6 +49,15 @@ typedef enum { PSTM_AMP_F32 = 0, PSTM_AMP_BF16 = 1, PSTM_AMP_F16 = 2 } pstm_amp_
  * traveltime (the precision form).  Weights and accumulation are FP32 in both. */
 typedef enum { PSTM_PREC_EXACT = 0, PSTM_PREC_FAST = 1 } pstm_precision;
 typedef enum { PSTM_IMAGE_F64 = 0, PSTM_IMAGE_F32 = 1 } pstm_image_dtype;
+
+/* Trace interpolators of pstm/kernels/interpolation.py:26-301 (linear is 0
+ * here, so a zeroed pstm_params interpolates linearly; the reference numbers
+ * nearest 0 and linear 1).  Non-linear methods run a separate FP64 kernel on
+ * the per-tile entry points. */
+typedef enum {
+    PSTM_INTERP_LINEAR = 0, PSTM_INTERP_NEAREST = 1, PSTM_INTERP_CUBIC = 2, PSTM_INTERP_SINC4 = 3,
+    PSTM_INTERP_SINC8 = 4, PSTM_INTERP_SINC16 = 5, PSTM_INTERP_LANCZOS3 = 6, PSTM_INTERP_LANCZOS5 = 7
+} pstm_interp;
 
 /* Traveltime kinds.  Reference: executor dispatch pstm/pipeline/executor.py:1691-1745
  * (migrate_tile / migrate_tile_curved_ray / migrate_tile_vti). */
@@ -113,7 +122,7 @@ typedef struct {
     int32_t compensated;          /* 1: compensated (TwoSum) FP32 accumulation */
     double eta_constant;
     int32_t precision;            /* pstm_precision; straight rays only, others are FP32 */
-    int32_t reserved;
+    int32_t interpolation;        /* pstm_interp; KernelConfig.interpolation_method, base.py:213 */
 } pstm_params;
 
 /* Library / ABI version (no reference counterpart: a binding sanity check). */

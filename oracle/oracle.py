@@ -47,7 +47,7 @@ class _Args(ctypes.Structure):
         ("curved_k", ctypes.c_double), ("eta", _dp), ("eta_is_3d", ctypes.c_int32),
         ("eta_constant", ctypes.c_double),
         ("pillar_begin", ctypes.c_int64), ("pillar_end", ctypes.c_int64),
-        ("n_threads", ctypes.c_int32),
+        ("n_threads", ctypes.c_int32), ("interp_method", ctypes.c_int32),
     ]
 
 
@@ -71,6 +71,8 @@ def lib():
         L.pstm_oracle_traveltime.restype = None
         L.pstm_oracle_linear_interp.argtypes = [_dp, ctypes.c_int32, ctypes.c_double]
         L.pstm_oracle_linear_interp.restype = ctypes.c_double
+        L.pstm_oracle_interp.argtypes = [_dp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32]
+        L.pstm_oracle_interp.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -161,7 +163,7 @@ def migrate(traces, output, velocity, config, kind=None, pillars=None, n_threads
         eta_constant=float(getattr(config, "vti_eta_constant", 0.0)),
         pillar_begin=0 if pillars is None else int(pillars[0]),
         pillar_end=0 if pillars is None else int(pillars[1]),
-        n_threads=int(n_threads),
+        n_threads=int(n_threads), interp_method=interp_code(getattr(config, "interpolation_method", None)),
     )
     rc = L.pstm_oracle_migrate(ctypes.byref(a))
     if rc != 0:
@@ -177,6 +179,25 @@ def traveltime(kind, feat7, v0=1500.0, k=0.5):
     out = np.empty(f.shape[0], np.float64)
     lib().pstm_oracle_traveltime(int(kind), f.shape[0], _p(f), float(v0), float(k), _p(out))
     return out
+
+
+# trace interpolators (names and aliases of pstm/kernels/interpolation.py:26-51)
+INTERP_BY_NAME = {"linear": 0, "nearest": 1, "cubic": 2, "sinc4": 3, "sinc8": 4, "sinc16": 5,
+                  "lanczos3": 6, "lanczos5": 7}
+INTERP_ALIASES = {"sinc": "sinc8", "spline": "cubic", "lanczos": "lanczos3"}
+
+
+def interp_code(name) -> int:
+    if name is None:
+        return 0
+    name = str(getattr(name, "value", name)).lower().strip()
+    return INTERP_BY_NAME[INTERP_ALIASES.get(name, name)]
+
+
+def interp(trace, t_sample, method):
+    """One interpolated sample by the restated reference interpolator."""
+    tr = np.ascontiguousarray(trace, dtype=np.float64)
+    return lib().pstm_oracle_interp(_p(tr), len(tr), float(t_sample), interp_code(method))
 
 
 def linear_interp(trace, t_sample):

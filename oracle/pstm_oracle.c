@@ -83,7 +83,19 @@ typedef struct {
        pillar_end <= 0 means all pillars */
     int64_t pillar_begin, pillar_end;
     int32_t n_threads;               /* <= 0: OpenMP default */
+    int32_t interp_method;           /* ORACLE_INTERP_* (0: linear) */
 } oracle_args;
+
+/* Trace interpolators of pstm/kernels/interpolation.py:59-285 (codes here put
+ * linear first; the reference numbers nearest 0 and linear 1). */
+#define ORACLE_INTERP_LINEAR   0
+#define ORACLE_INTERP_NEAREST  1
+#define ORACLE_INTERP_CUBIC    2
+#define ORACLE_INTERP_SINC4    3
+#define ORACLE_INTERP_SINC8    4
+#define ORACLE_INTERP_SINC16   5
+#define ORACLE_INTERP_LANCZOS3 6
+#define ORACLE_INTERP_LANCZOS5 7
 
 /* straight-ray one-way leg, numba_cpu_optimized.py:192-194 */
 static double leg_straight(double t0h2, double h2, double inv_v2)
@@ -160,10 +172,22 @@ static double aa_weight(double ox, double oy, double mx, double my, double v,
     return w > 0.0 ? w : 0.0;
 }
 
+typedef struct {
+    const oracle_args *a;
+    int64_t tr;
+} trace_ref;
+static double interp_sample(double (*get)(const void *, int64_t), const void *ctx, int32_t n, double t, int32_t m);
+
 static inline double amp_at(const oracle_args *a, int64_t tr, int64_t i)
 {
     if (a->amp_is_f64) return ((const double *)a->amplitudes)[tr * a->n_samples + i];
     return (double)((const float *)a->amplitudes)[tr * a->n_samples + i];
+}
+
+static double trace_get(const void *p, int64_t i)
+{
+    const trace_ref *r = (const trace_ref *)p;
+    return amp_at(r->a, r->tr, i);
 }
 
 /*
@@ -257,9 +281,15 @@ int pstm_oracle_migrate(const oracle_args *a)
                     }
                     const double s = (T - tstart_s) / dt_s;
                     if (s < 0.0 || s >= (double)(ns - 1)) continue;
-                    const int64_t i0 = (int64_t)s;
-                    const double f = s - (double)i0;
-                    const double amp = amp_at(a, tr, i0) * (1.0 - f) + amp_at(a, tr, i0 + 1) * f;
+                    double amp;
+                    if (a->interp_method == ORACLE_INTERP_LINEAR) {
+                        const int64_t i0 = (int64_t)s;
+                        const double f = s - (double)i0;
+                        amp = amp_at(a, tr, i0) * (1.0 - f) + amp_at(a, tr, i0 + 1) * f;
+                    } else {
+                        const trace_ref r = {a, tr};
+                        amp = interp_sample(trace_get, &r, ns, s, a->interp_method);
+                    }
                     double w = wtr;
                     const double ts = apt * (1.0 - tap);
                     if (dmid > ts) {
@@ -318,6 +348,67 @@ void pstm_oracle_traveltime(int32_t kind, int64_t n, const double *feat7,
         }
         out[i] = T;
     }
+}
+
+/* sin(pi x)/(pi x), 1 at x ~ 0 (interpolation.py:139-144) */
+static double sinc_pi(double x)
+{
+    if (fabs(x) < 1e-10) return 1.0;
+    return sin(M_PI * x) / (M_PI * x);
+}
+
+/* One sample of `trace` (n samples, read through get(i)) at fractional index t:
+ * nearest (:59-66), linear (:68-92), Catmull-Rom cubic (:95-135), Hanning-
+ * windowed sinc of half-width 2/4/8 (:147-189), Lanczos 3/5 (:208-249); the
+ * higher-order methods fall back to linear within their half-width of an end
+ * and normalise by the sum of their weights. */
+static double interp_sample(double (*get)(const void *, int64_t), const void *ctx, int32_t n, double t, int32_t m)
+{
+    if (m == ORACLE_INTERP_NEAREST) {
+        const int64_t i = (int64_t)(t + 0.5);
+        return (i < 0 || i >= n) ? 0.0 : get(ctx, i);
+    }
+    const int hw = m == ORACLE_INTERP_SINC4 ? 2 : m == ORACLE_INTERP_SINC8 ? 4 : m == ORACLE_INTERP_SINC16 ? 8
+                 : m == ORACLE_INTERP_LANCZOS3 ? 3 : m == ORACLE_INTERP_LANCZOS5 ? 5 : 0;
+    const int cubic_edge = m == ORACLE_INTERP_CUBIC && (t < 1.0 || t >= (double)(n - 2));
+    const int wide_edge = hw > 0 && (t < (double)hw || t >= (double)(n - hw));
+    if (m == ORACLE_INTERP_LINEAR || cubic_edge || wide_edge) {
+        if (t < 0.0 || t >= (double)(n - 1)) return 0.0;
+        const int64_t i0 = (int64_t)t;
+        const double f = t - (double)i0;
+        return get(ctx, i0) * (1.0 - f) + get(ctx, i0 + 1) * f;
+    }
+    if (m == ORACLE_INTERP_CUBIC) {
+        const int64_t i = (int64_t)t;
+        const double u = t - (double)i;
+        const double p0 = get(ctx, i - 1), p1 = get(ctx, i), p2 = get(ctx, i + 1), p3 = get(ctx, i + 2);
+        const double c3 = -0.5 * p0 + 1.5 * p1 - 1.5 * p2 + 0.5 * p3;
+        const double c2 = p0 - 2.5 * p1 + 2.0 * p2 - 0.5 * p3;
+        const double c1 = -0.5 * p0 + 0.5 * p2;
+        return ((c3 * u + c2) * u + c1) * u + p1;
+    }
+    const int lanczos = m == ORACLE_INTERP_LANCZOS3 || m == ORACLE_INTERP_LANCZOS5;
+    const int64_t ic = lanczos ? (int64_t)t : (int64_t)(t + 0.5);
+    const double frac = t - (double)ic;
+    double acc = 0.0, norm = 0.0;
+    for (int k = -hw + 1; k <= hw; ++k) {
+        const int64_t i = ic + k;
+        if (i < 0 || i >= n) continue;
+        const double x = frac - (double)k;
+        double w;
+        if (lanczos) w = fabs(x) < 1e-10 ? 1.0 : (fabs(x) >= hw ? 0.0 : sinc_pi(x) * sinc_pi(x / hw));
+        else w = sinc_pi(x) * (fabs(x) >= hw ? 0.0 : 0.5 * (1.0 + cos(M_PI * x / hw)));
+        acc += get(ctx, i) * w;
+        norm += w;
+    }
+    return norm > 1e-10 ? acc / norm : 0.0;
+}
+
+static double get_f64(const void *p, int64_t i) { return ((const double *)p)[i]; }
+
+double pstm_oracle_interp(const double *trace, int32_t n, double t_sample, int32_t method)
+{
+    return interp_sample(get_f64, trace, n, t_sample, method);
 }
 
 /* The reference's linear interpolator, pstm/kernels/interpolation.py:68-92. */

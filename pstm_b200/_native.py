@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpstm_cuda.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # pstm_status
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_INITIALIZED, \
@@ -27,6 +27,21 @@ AMP_F32, AMP_BF16, AMP_F16 = 0, 1, 2
 IMAGE_F64, IMAGE_F32 = 0, 1
 TT_STRAIGHT, TT_CURVED, TT_VTI, TT_CURVED_VTI = 0, 1, 2, 3
 PREC_EXACT, PREC_FAST = 0, 1
+# pstm_interp, named as KernelConfig.interpolation_method (aliases of interpolation.py:42-51)
+INTERP_BY_NAME = {"linear": 0, "nearest": 1, "cubic": 2, "sinc4": 3, "sinc8": 4, "sinc16": 5,
+                  "lanczos3": 6, "lanczos5": 7}
+INTERP_ALIASES = {"sinc": "sinc8", "spline": "cubic", "lanczos": "lanczos3"}
+
+
+def interp_code(name) -> int:
+    """pstm_interp code of an interpolation method name or enum (None: linear)."""
+    if name is None:
+        return 0
+    key = str(getattr(name, "value", name)).lower().strip()
+    key = INTERP_ALIASES.get(key, key)
+    if key not in INTERP_BY_NAME:
+        raise ValueError(f"unknown interpolation method {name!r}")
+    return INTERP_BY_NAME[key]
 STREAM_LEGACY = 1   # cudaStreamLegacy
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -64,7 +79,7 @@ class Params(ctypes.Structure):
         ("aa_dominant_freq", ctypes.c_double), ("grid_dx", ctypes.c_double),
         ("grid_dy", ctypes.c_double), ("curved_v0", ctypes.c_double), ("curved_k", ctypes.c_double),
         ("eta", _vp), ("eta_is_3d", ctypes.c_int32), ("compensated", ctypes.c_int32),
-        ("eta_constant", ctypes.c_double), ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("eta_constant", ctypes.c_double), ("precision", ctypes.c_int32), ("interpolation", ctypes.c_int32),
     ]
 
 

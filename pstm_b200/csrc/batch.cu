@@ -99,6 +99,8 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     o.fold = nullptr;
     const char *msg = "";
     if ((rc = plan::check_args(tr, &o, vel, prm, msg)) != PSTM_OK) return fail(c, rc, msg);
+    if (prm->interpolation != PSTM_INTERP_LINEAR)
+        return fail(c, PSTM_ERR_UNSUPPORTED, "the batched form interpolates linearly");
     for (int i = 0; i < n_bins; ++i)
         if (bins[i].n_traces > 0)
             bp.work.push_back({bins[i].trace_begin, bins[i].n_traces, bins[i].image, bins[i].fold});

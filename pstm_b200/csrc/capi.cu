@@ -187,6 +187,7 @@ int32_t run_dev(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out,
     TilePlan tp;
     const int32_t rc = prepare_tile(c, tr, out, vel, prm, st, tp);
     if (rc || tp.empty) return rc;
+    if (prm->interpolation != PSTM_INTERP_LINEAR) return launch_interp(c, tp, prm->interpolation, out);
     return launch_tile(c, tp);
 }
 

@@ -58,6 +58,7 @@ struct TilePlan {
 int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *out, const pstm_velocity_desc *vel,
                      const pstm_params *prm, cudaStream_t st, TilePlan &tp);
 int32_t launch_tile(Ctx *c, const TilePlan &tp);
+int32_t launch_interp(Ctx *c, const TilePlan &tp, int method, const pstm_output_desc *out);   // interp.cu
 int32_t check_error_word(Ctx *c);   // after the stream has drained
 
 int32_t fail(Ctx *c, int32_t code, const std::string &msg);

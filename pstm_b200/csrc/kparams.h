@@ -80,6 +80,7 @@ struct KParams {
     int32_t spreading, obliquity;
     int32_t aa;
     float aa_cA, aa_cB;          // 4*max(dx,dy)*f_dom, f_dom/500
+    double aa_gmax, aa_fdom;     // max(dx, dy), f_dom (FP64 paths)
     double cr_v0, cr_k;
     float cr_v0f, cr_kf, cr_inv_k_ln2;   // inv_k * ln2 (log2 based)
     int32_t cr_k_zero;           // |k| < 1e-10: straight-ray fallback with v0

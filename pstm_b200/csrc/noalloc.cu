@@ -97,6 +97,8 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     const char *msg = "";
     int32_t rc = plan::check_args(tr, out, vel, prm, msg);
     if (rc) return fail(rc, msg);
+    if (prm->interpolation != PSTM_INTERP_LINEAR)
+        return fail(PSTM_ERR_UNSUPPORTED, "the allocation-free entry point interpolates linearly");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");

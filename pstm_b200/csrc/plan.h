@@ -54,6 +54,8 @@ inline int32_t check_args(const pstm_traces_desc *tr, const pstm_output_desc *ou
         return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown traveltime kind");
     if (prm->precision != PSTM_PREC_EXACT && prm->precision != PSTM_PREC_FAST)
         return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (prm->interpolation < PSTM_INTERP_LINEAR || prm->interpolation > PSTM_INTERP_LANCZOS5)
+        return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown interpolation method");
     if (!(prm->max_aperture_m >= 0.0) || !(prm->taper_fraction >= 0.0) || !(prm->taper_fraction <= 1.0))
         return fail(PSTM_ERR_INVALID_ARGUMENT, "bad aperture/taper parameters");
     if ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) && !(prm->curved_v0 > 0.0))
@@ -116,6 +118,8 @@ inline KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *o
     const double gmax = prm->grid_dx > prm->grid_dy ? prm->grid_dx : prm->grid_dy;
     P.aa_cA = (float)(4.0 * gmax * prm->aa_dominant_freq);
     P.aa_cB = (float)(prm->aa_dominant_freq / 500.0);
+    P.aa_gmax = gmax;
+    P.aa_fdom = prm->aa_dominant_freq;
     P.cr_v0 = prm->curved_v0;
     P.cr_k = prm->curved_k;
     P.cr_v0f = (float)prm->curved_v0;

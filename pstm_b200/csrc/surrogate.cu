@@ -572,6 +572,8 @@ int32_t pstm_cuda_migrate_tile_learned_dev(void *ctx, const pstm_traces_desc *tr
     if (rc) return rc;
     if (!params || !report) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "null descriptor");
     std::memset(report, 0, sizeof(*report));
+    if (params->interpolation != PSTM_INTERP_LINEAR)
+        return fail(c, PSTM_ERR_UNSUPPORTED, "the learned form interpolates linearly");
     if (params->traveltime != net->traveltime)
         return fail(c, PSTM_ERR_INVALID_ARGUMENT, "the surrogate was trained for another traveltime kind");
     if (n_probe < 32) n_probe = 32;

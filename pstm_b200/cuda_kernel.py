@@ -279,6 +279,7 @@ class CudaKernel:
         p.eta_constant = float(getattr(cfg, "vti_eta_constant", 0.0))
         p.compensated = int(self._compensated)
         p.precision = self._precision
+        p.interpolation = nat.interp_code(getattr(cfg, "interpolation_method", None))
         eta = eta_override if eta_override is not None else getattr(cfg, "vti_eta_array", None)
         if eta is not None and tt in (nat.TT_VTI, nat.TT_CURVED_VTI):
             ptr, on_dev = self._arr(eta, np.float64, keep)

@@ -87,3 +87,15 @@ def test_oracle_rejects_bad_arguments():
     case.traces.amplitudes = case.traces.amplitudes[:, :1]   # fewer than 2 samples
     with pytest.raises(ValueError):
         oracle.migrate(case.traces, case.output, case.velocity, case.config)
+
+
+def test_oracle_interpolators_match_reference_golden():
+    """Every trace interpolator of the oracle against the reference's own
+    interpolate_sample (tests/golden/interp_methods.npz)."""
+    z = np.load(os.path.join(GOLDEN, "interp_methods.npz"))
+    codes = dict(zip(z["method_names"], z["reference_codes"]))
+    for name in z["method_names"]:
+        for i, tr in enumerate(z["traces"]):
+            for j, t in enumerate(z["t_samples"]):
+                got = oracle.interp(tr, t, str(name))
+                assert abs(got - z["values"][codes[name], i, j]) <= 1e-12, (name, i, t)
