@@ -230,9 +230,10 @@ def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, 
     n_acc = 1 << 16
     amps_host = amps[:n_acc].float().cpu().numpy()
     res = {}
-    specs = [("plain_exact_f32", "f32", "exact"), ("precision_bf16_fast", "bf16", "fast")]
+    specs = [("plain_exact_f32", "f32", "exact"), ("precision_bf16_fast", "bf16", "fast"),
+             ("precision_f16_fast", "f16", "fast")]
     for name, dt, prec in specs:
-        tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[dt]
+        tdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[dt]
         tbf = tb if (dt == args.dtype and tdt == amps.dtype) else dataclasses.replace(tb, amplitudes=amps.to(tdt))
         kf = CudaKernel(precision=prec)
         kf.initialize(cfg)
