@@ -223,7 +223,8 @@ std::vector<unsigned char> graph_key(const BatchPlan &bp) {
     };
     put(&bp.P, sizeof(KParams));
     if (!bp.work.empty()) put(bp.work.data(), bp.work.size() * sizeof(BinWork));
-    const int64_t extra[6] = {bp.tt, bp.amp, bp.per_pillar, bp.exact, (int64_t)bp.L.grid.x, (int64_t)bp.L.smem};
+    const int64_t extra[8] = {bp.tt, bp.amp, bp.per_pillar, bp.exact, (int64_t)bp.L.grid.x, (int64_t)bp.L.smem,
+                              (int64_t)(uintptr_t)bp.L.bins, (int64_t)(uintptr_t)bp.L.counter};
     put(extra, sizeof(extra));
     return k;
 }
@@ -281,6 +282,8 @@ void release_batch(Ctx *c) {
     release(c->tune_image);
     release(c->tune_fold);
     release(c->probe);
+    release(c->seg_bins);
+    release(c->seg_counter);
 }
 }  // namespace ctx
 }  // namespace pstm

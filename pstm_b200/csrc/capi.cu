@@ -172,7 +172,43 @@ int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc 
     return PSTM_OK;
 }
 
+// A panel much larger than L2 is migrated segment by segment: the persistent
+// kernel takes items (trace segment, pillar block, time block) in segment
+// order, so every resident CTA streams the same L2-sized segment at a time
+// and the panel is read from DRAM about once instead of once per CTA; the
+// items of a pillar block in different segments add into the image and fold
+// atomically.
 int32_t launch_tile(Ctx *c, const TilePlan &tp) {
+    const KParams &P0 = tp.P;
+    const int64_t row_bytes = (int64_t)P0.pitch * P0.elem;
+    if (c->segment_bytes > 0 && P0.n_traces * row_bytes > 2 * c->segment_bytes) {
+        int64_t S = c->segment_bytes / row_bytes;
+        S = S < 16 * (int64_t)P0.chunk ? 16 * (int64_t)P0.chunk : S / P0.chunk * P0.chunk;
+        const int64_t nseg = (P0.n_traces + S - 1) / S;
+        std::vector<BinWork> w((size_t)nseg);
+        for (int64_t i = 0; i < nseg; ++i) {
+            const int64_t b = i * S;
+            w[(size_t)i] = {b, (P0.n_traces - b) < S ? (P0.n_traces - b) : S, P0.image, P0.fold};
+        }
+        cudaError_t e;
+        if ((e = ensure(c->seg_bins, w.size() * sizeof(BinWork))) != cudaSuccess ||
+            (e = ensure(c->seg_counter, sizeof(unsigned long long))) != cudaSuccess)
+            return cuda_fail(c, e, "allocating the segment list");
+        if ((e = cudaMemcpyAsync(c->seg_bins.ptr, w.data(), w.size() * sizeof(BinWork), cudaMemcpyHostToDevice,
+                                 tp.L.stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(c->seg_counter.ptr, 0, sizeof(unsigned long long), tp.L.stream)) != cudaSuccess)
+            return cuda_fail(c, e, "writing the segment list");
+        KParams P = P0;
+        P.atomic_flush = 1;
+        Launch L;
+        L.smem = tp.L.smem;
+        L.stream = tp.L.stream;
+        L.bins = reinterpret_cast<const BinWork *>(c->seg_bins.ptr);
+        L.n_bins = (int)nseg;
+        L.counter = reinterpret_cast<unsigned long long *>(c->seg_counter.ptr);
+        e = launch_kind(tp.tt, P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, L);
+        return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "segmented migrate kernel launch");
+    }
     const cudaError_t e = launch_kind(tp.tt, tp.P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, tp.L);
     return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "migrate kernel launch");
 }
@@ -252,6 +288,8 @@ int32_t pstm_cuda_create(int32_t device, void **ctx_out) {
     if (rr) c->force_r = std::atoi(rr);
     const char *pb = std::getenv("PSTM_CUDA_PB");   // pillars per CTA override (1..16)
     if (pb) c->force_pb = std::atoi(pb);
+    const char *seg = std::getenv("PSTM_CUDA_SEGMENT_MB");   // trace-segment size; 0: never split a panel
+    if (seg) c->segment_bytes = (int64_t)std::atoll(seg) << 20;
     *ctx_out = c;
     return PSTM_OK;
 }

@@ -40,6 +40,7 @@ struct KParams {
     // ---- staging of trace rows in shared memory ----
     int32_t chunk;               // traces per chunk (<= kMaxChunk)
     int32_t n_tblk;              // time blocks per output (persistent form)
+    int32_t atomic_flush;        // outputs shared by concurrent items: atomic image/fold adds
     int32_t pb;                  // pillars per CTA (<= kMaxPB)
     int32_t r_per_lane;          // output times per lane (R)
     int32_t pitch;               // staged row pitch, elements (multiple of 16 bytes)

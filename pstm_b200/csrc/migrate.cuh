@@ -559,8 +559,14 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 float &a = s_acc[(q * R + r) * kThreads + tid];
                 if (p >= 0 && t < P.nt && a != 0.f) {
                     const int64_t idx = (int64_t)p * P.nt + t;
-                    if (P.image_f32) reinterpret_cast<float *>(it.image)[idx] += a;
-                    else reinterpret_cast<double *>(it.image)[idx] += (double)a;
+                    if (P.atomic_flush) {   // items of several trace segments share the outputs
+                        if (P.image_f32) atomicAdd(reinterpret_cast<float *>(it.image) + idx, a);
+                        else atomicAdd(reinterpret_cast<double *>(it.image) + idx, (double)a);
+                    } else if (P.image_f32) {
+                        reinterpret_cast<float *>(it.image)[idx] += a;
+                    } else {
+                        reinterpret_cast<double *>(it.image)[idx] += (double)a;
+                    }
                 }
                 a = 0.f;
             }
@@ -749,13 +755,20 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int t = t_lane + r * kThreads;
-                if (t < P.nt) it.fold[(int64_t)p * P.nt + t] += cnt;
+                if (t < P.nt) {
+                    int32_t *f = it.fold + (int64_t)p * P.nt + t;
+                    if (P.atomic_flush) atomicAdd(f, cnt);
+                    else *f += cnt;
+                }
             }
         }
     }
     if (it.fold && !P.fold3d && it.tblock == 0 && tid < PB) {
         const int p = s_pid[tid];
-        if (p >= 0) it.fold[p] += s_fold[tid];
+        if (p >= 0) {
+            if (P.atomic_flush) atomicAdd(it.fold + p, s_fold[tid]);
+            else it.fold[p] += s_fold[tid];
+        }
     }
     return true;
 }
