@@ -46,9 +46,9 @@ FLOP_PER_PAIR = 20
 MUFU_PER_PAIR = 4
 
 # DRAM traffic of one 64 x 64 x 1500 tile launch per trace of the panel, from an
-# ncu capture (dram__bytes) of the same launch at 32,768 traces: 5.04 GB; the
-# traffic grows in proportion to the traces streamed
-DRAM_BYTES_PER_TRACE_TILE64 = 5.04e9 / 32768
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of the
+# full-size launch (1,048,576 traces, 24 MiB trace segments): 63.3 + 19.3 GB
+DRAM_BYTES_PER_TRACE_TILE64 = 82.6e9 / 1048576
 
 
 def parse():
@@ -621,7 +621,7 @@ def main_ours(args):
         "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
                 "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes},
         "traffic": (DRAM_BYTES_PER_TRACE_TILE64 * N / 1e9) if T == 64 else None,
-        "traffic_unit": "GB per launch (ncu dram__bytes at 32,768 traces, scaled by traces)",
+        "traffic_unit": "GB per launch (ncu dram__bytes read+write of the full-size launch, scaled by traces)",
     }
 
     # ---- end to end through the public API with pinned host buffers

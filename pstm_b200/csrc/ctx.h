@@ -39,7 +39,7 @@ struct Ctx {
     DevBuf bins, counter, tune_image, tune_fold;
     DevBuf probe;                           // learned form: per-probe residuals
     DevBuf seg_bins, seg_counter;           // per-tile launches split into trace segments
-    int64_t segment_bytes = 48ll << 20;     // trace-panel bytes per segment (0: never split)
+    int64_t segment_bytes = 24ll << 20;     // trace-panel bytes per segment (0: never split)
     std::vector<unsigned char> graph_key;   // arguments the cached graph was captured with
     cudaGraphExec_t graph = nullptr;
     std::map<std::string, Shape> tuned;     // autotuned shapes by workload class
