@@ -155,6 +155,30 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     if (!plan::plan_staging(P, tr, prm, PB, R, c->smem_optin, smem, chunk))
         return fail(c, PSTM_ERR_UNSUPPORTED, "trace rows too long to stage in shared memory");
 
+    // bins much larger than L2 are split into trace segments (consecutive in the
+    // work list, so the resident CTAs share each segment in L2); split bins add
+    // into their outputs atomically
+    const int64_t row_bytes = (int64_t)P.pitch * P.elem;
+    if (c->segment_bytes > 0) {
+        int64_t S = c->segment_bytes / row_bytes;
+        S = S < 16 * (int64_t)P.chunk ? 16 * (int64_t)P.chunk : S / P.chunk * P.chunk;
+        std::vector<BinWork> split;
+        for (const BinWork &w : bp.work) {
+            if (w.n_traces * row_bytes <= 2 * c->segment_bytes) {
+                split.push_back(w);
+                continue;
+            }
+            for (int64_t b = 0; b < w.n_traces; b += S)
+                split.push_back({w.trace0 + b, (w.n_traces - b) < S ? (w.n_traces - b) : S, w.image, w.fold});
+            P.atomic_flush = 1;
+        }
+        if (split.size() > (size_t)(64 * kMaxBins))
+            return fail(c, PSTM_ERR_UNSUPPORTED, "too many trace segments in one batch");
+        bp.work.swap(split);
+        if ((e = ensure(c->bins, bp.work.size() * sizeof(BinWork))) != cudaSuccess)
+            return cuda_fail(c, e, "allocating the batch work list");
+    }
+
     bp.L = Launch();
     bp.L.smem = smem;
     bp.L.bins = reinterpret_cast<const BinWork *>(c->bins.ptr);
