@@ -151,6 +151,7 @@ struct PtState {
     float K;               // weight numerator
     float ivw_t;           // 1/v_w per unit of T (AA sin theta)
     float aaA;             // 4 max(dx,dy) f_dom / v_w (AA)
+    float aa_k, aa_thr;    // aaA / v_w per unit of T; minf / T above which sin(theta) >= 0.01
     float t02v2, c1, e2;   // VTI: (t0/2)^2 v^2, 1+2eta, 2 eta / v^2
     double B;              // EXACT: 1/(v dt)^2
 };
@@ -192,6 +193,8 @@ __device__ __forceinline__ void load_states(const KParams &P, int p, int t, Time
     // T is in seconds, or in samples on the EXACT path: 1/(v T_sec) = (1/(v dt)) / T_samples
     s.ivw_t = EXACT ? ivw * P.inv_dt_f : ivw;
     s.aaA = P.aa_cA * ivw;
+    s.aa_k = s.aaA * s.ivw_t;
+    s.aa_thr = 0.01f * rcp_approx(s.ivw_t);
     s.K = P.spreading ? ts.Kt * s.ivw_t : ts.Kt;
     s.t02v2 = 0.f;
     s.c1 = 1.f;
@@ -301,7 +304,7 @@ static __device__ __noinline__ bool exact_outside_aperture(const KParams *P, int
 }
 
 // ---------------------------------------------------------------- traveltime (FP32)
-// Records: A = {d, wt, minf, trace slot}; B = {ds2, dr2, k^2 ds2 | ds2^2, k^2 dr2 | dr2^2};
+// Records: A = {d, wt, minf, byte offset of the trace's staged row}; B = {ds2, dr2, k^2 ds2 | ds2^2, k^2 dr2 | dr2^2};
 // C (curved kinds) = {1/(bs br) | 1/bs, 1/br, ds2^2, dr2^2}.  Result in seconds.
 template <int TT>
 __device__ __forceinline__ float traveltime(const KParams &P, const TimeState &ts, const PtState &s,
@@ -471,7 +474,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             const int p = s_pid[q];
             bool in = false;
             const float inf = __int_as_float(0x7f800000);
-            float4 A = make_float4(inf, 0.f, 0.f, __int_as_float(c));
+            float4 A = make_float4(inf, 0.f, 0.f, __int_as_float(c * row_bytes));
             float4 Bf = make_float4(0.f, 0.f, 0.f, 0.f), Cc = Bf;
             double2 B64 = make_double2(0.0, 0.0);
             if (p >= 0 && c < cmax) {
@@ -486,7 +489,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     const double ds2 = dxs * dxs + dys * dys, dr2 = dxr * dxr + dyr * dyr;
                     // the FP64 sqrt is needed only where the aperture cut is hard
                     const float d = hard_cut ? (float)sqrt(d2) : sqrt_approx((float)d2);
-                    A = make_float4(d, (float)g[6], (float)fmax(fabs(dxm), fabs(dym)), __int_as_float(c));
+                    A = make_float4(d, (float)g[6], (float)fmax(fabs(dxm), fabs(dym)), __int_as_float(c * row_bytes));
                     B64 = make_double2(ds2, dr2);
                     Bf = make_float4((float)ds2, (float)dr2, 0.f, 0.f);
                     if constexpr (TT == TT_CURVED || TT == TT_CURVED_VTI) {
@@ -627,9 +630,9 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     const int ri = q * kMaxChunk + c;
                     const float4 A = recA[ri];
                     bool act = A.x <= s.ap;
-                    const int slot = __float_as_int(A.w);
+                    const int roff = __float_as_int(A.w);   // row offset; the trace is roff / row_bytes
                     if (HARD && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
-                        act = !exact_outside_aperture(Pg, it.trace0 + c0 + slot, p, t, s_ox[q], s_oy[q]);
+                        act = !exact_outside_aperture(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q], s_oy[q]);
                     float T, f;
                     int i0;
                     bool ok;
@@ -656,7 +659,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         const bool band = act && !fast_ok && !ts.tz && sidx >= sr_lo && sidx <= sr_hi;
                         if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
                         if constexpr (SLOW) {   // re-decide the guard band in FP64
-                            ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + slot, p, t, s_ox[q], s_oy[q]);
+                            ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q],
+                                                             s_oy[q]);
                             sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
                         } else {
                             ok = act && fast_ok;
@@ -667,7 +671,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         i0 = __float_as_int(fl) - 0x4B000000;
                         f = sidx - (fl - 8388608.f);
                     }
-                    const unsigned char *row = ampb + slot * row_bytes;
+                    const unsigned char *row = ampb + roff;
                     const float a0 = amp_at<AMP>(row, i0);
                     const float a1 = amp_at<AMP>(row, i0 + 1);
                     const float amp = fmaf(f, a1 - a0, a0);
@@ -682,9 +686,10 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     else gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
                     gw = T > ts.tg ? gw : 1.f;   // the reference applies them only for T > 1 ms
                     if (aa_on) {
-                        const float sth = fminf(A.z * s.ivw_t * rT, 1.f);
-                        const float aa = fmaxf(0.f, 1.f - fmaxf(s.aaA * sth, aa_cB));
-                        gw = (sth >= 0.01f && T >= ts.tguard) ? gw * aa : gw;
+                        // sin(theta) = min(minf / (v_w T), 1); aaA sin(theta) = min(u aaA / v_w, aaA)
+                        const float u = A.z * rT;
+                        const float aa = fmaxf(0.f, 1.f - fmaxf(fminf(u * s.aa_k, s.aaA), aa_cB));
+                        gw = (u >= s.aa_thr && T >= ts.tguard) ? gw * aa : gw;
                     }
                     return amp * (w * gw);
                 };
