@@ -623,10 +623,14 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 unsigned pmask = 0u;   // FP32 path: records with a pair in a trace-end guard band
 
                 // contribution of record c (slot in the sorted order) to this lane's time
-                auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c) -> float {
+                // CHK: some lane of the warp may have T <= 1 ms (t0 < 1.1 ms, or curved rays),
+                // so the "T > 1 ms" conditions of the weights are evaluated; otherwise every
+                // T of the warp exceeds t0 >= 1.1 ms and they are known to hold
+                auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c, auto chk_c) -> float {
                     constexpr bool TAPER = decltype(taper_c)::value;
                     constexpr bool SLOW = decltype(slow_c)::value;
                     constexpr bool HARD = decltype(hard_c)::value;
+                    constexpr bool CHK = decltype(chk_c)::value;
                     const int ri = q * kMaxChunk + c;
                     const float4 A = recA[ri];
                     bool act = A.x <= s.ap;
@@ -684,33 +688,39 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     float gw;
                     if constexpr (W2) gw = s.K * rT * rT;
                     else gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
-                    gw = T > ts.tg ? gw : 1.f;   // the reference applies them only for T > 1 ms
+                    if constexpr (CHK) gw = T > ts.tg ? gw : 1.f;   // the reference applies them only for T > 1 ms
                     if (aa_on) {
                         // sin(theta) = min(minf / (v_w T), 1); aaA sin(theta) = min(u aaA / v_w, aaA)
                         const float u = A.z * rT;
                         const float aa = fmaxf(0.f, 1.f - fmaxf(fminf(u * s.aa_k, s.aaA), aa_cB));
-                        gw = (u >= s.aa_thr && T >= ts.tguard) ? gw * aa : gw;
+                        gw = (u >= s.aa_thr && (!CHK || T >= ts.tguard)) ? gw * aa : gw;
                     }
                     return amp * (w * gw);
                 };
                 using F = std::false_type;
                 using Tr = std::true_type;
                 float a = 0.f;
+                const bool small_t = __any_sync(0xffffffffu, ts.tg >= 0.f);
                 if (!hard_cut) {
-                    PSTM_UNROLL(PSTM_UNROLL_PLAIN)
-                    for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{});
+                    if (small_t) {
+                        PSTM_UNROLL(PSTM_UNROLL_TAPER)
+                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, Tr{});
+                    } else {
+                        PSTM_UNROLL(PSTM_UNROLL_PLAIN)
+                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, F{});
+                    }
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{});
+                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, Tr{});
                 } else {   // no taper: the aperture edge is a hard cut, ties are decided in FP64
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                    for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{});
+                    for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{}, Tr{});
                 }
                 if constexpr (!EXACT) {   // second pass over the flagged records only
                     unsigned m = __reduce_or_sync(0xffffffffu, pmask);
                     while (m) {
                         const int c = __ffs(m) - 1;
                         m &= m - 1u;
-                        a += pair(c, Tr{}, Tr{}, Tr{});
+                        a += pair(c, Tr{}, Tr{}, Tr{}, Tr{});
                     }
                 }
                 s_acc[(q * R + r) * kThreads + tid] += a;
