@@ -616,7 +616,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 // records inside the aperture of some lane: a prefix of length n;
                 // records with no lane in its taper band: a prefix of length n0
                 const float apw = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(s.ap)));
-                const float tsl = s.ap > 0.f ? s.ap * one_m_taper : __int_as_float(0x7f800000);
+                // lanes past the tile end (ap < 0) take no part; a zero aperture gives 0
+                const float tsl = s.ap >= 0.f ? s.ap * one_m_taper : __int_as_float(0x7f800000);
                 const float tmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(tsl)));
                 const int n = __popc(__ballot_sync(0xffffffffu, dl <= apw));
                 const int n0 = min(n, __popc(__ballot_sync(0xffffffffu, dl <= tmin)));
@@ -626,14 +627,17 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 // CHK: some lane of the warp may have T <= 1 ms (t0 < 1.1 ms, or curved rays),
                 // so the "T > 1 ms" conditions of the weights are evaluated; otherwise every
                 // T of the warp exceeds t0 >= 1.1 ms and they are known to hold
-                auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c, auto chk_c) -> float {
+                // ALLIN: the record is inside every valid lane's aperture (c < n0), so the
+                // aperture test is known to pass
+                auto pair = [&](int c, auto taper_c, auto slow_c, auto hard_c, auto chk_c, auto allin_c) -> float {
                     constexpr bool TAPER = decltype(taper_c)::value;
                     constexpr bool SLOW = decltype(slow_c)::value;
                     constexpr bool HARD = decltype(hard_c)::value;
                     constexpr bool CHK = decltype(chk_c)::value;
+                    constexpr bool ALLIN = decltype(allin_c)::value;
                     const int ri = q * kMaxChunk + c;
                     const float4 A = recA[ri];
-                    bool act = A.x <= s.ap;
+                    bool act = ALLIN ? true : (A.x <= s.ap);
                     const int roff = __float_as_int(A.w);   // row offset; the trace is roff / row_bytes
                     if (HARD && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
                         act = !exact_outside_aperture(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q], s_oy[q]);
@@ -704,23 +708,23 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 if (!hard_cut) {
                     if (small_t) {
                         PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, Tr{});
+                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, Tr{}, Tr{});
                     } else {
                         PSTM_UNROLL(PSTM_UNROLL_PLAIN)
-                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, F{});
+                        for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, F{}, Tr{});
                     }
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, Tr{});
+                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, Tr{}, F{});
                 } else {   // no taper: the aperture edge is a hard cut, ties are decided in FP64
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                    for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{}, Tr{});
+                    for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{}, Tr{}, F{});
                 }
                 if constexpr (!EXACT) {   // second pass over the flagged records only
                     unsigned m = __reduce_or_sync(0xffffffffu, pmask);
                     while (m) {
                         const int c = __ffs(m) - 1;
                         m &= m - 1u;
-                        a += pair(c, Tr{}, Tr{}, Tr{}, Tr{});
+                        a += pair(c, Tr{}, Tr{}, Tr{}, Tr{}, F{});
                     }
                 }
                 s_acc[(q * R + r) * kThreads + tid] += a;
