@@ -1,7 +1,7 @@
 """Generate golden fixtures by running the reference implementation.
 
 Run in a container where the reference project is importable (it is read
-from REF, default /root/reference); the GPU box never runs this.  Writes
+from REF, default /root/reference); the tests read only its output.  Writes
 ``*.npz`` next to this file:
 
 * ``numba_*.npz``   inputs and outputs of the reference's registered CPU
