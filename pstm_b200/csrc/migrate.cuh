@@ -429,7 +429,10 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
 
     // hot-loop constants in registers
     const float s_scale = P.s_scale, s_offset = P.s_offset;
-    const float sg_lo = P.s_guard_lo, sg_hi = P.s_guard_hi, sr_lo = P.s_rej_lo, sr_hi = P.s_rej_hi;
+    // guard bands around the trace ends, as distances from the middle of the trace:
+    // |s - mid| <= g_in is inside by more than the band, g_in < |s - mid| <= g_out is in a band
+    const float g_mid = 0.5f * (P.s_guard_lo + P.s_guard_hi);
+    const float g_in = P.s_guard_hi - g_mid, g_out = P.s_rej_hi - g_mid;
     const float s_clamp = P.s_max_clamp;
     const unsigned ns_m1 = (unsigned)(P.ns - 1);
     const double magic = P.s_magic;
@@ -663,8 +666,9 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         if constexpr (TT != TT_STRAIGHT) T = ts.tz ? 0.f : T;
                         float sidx = fmaf(T, s_scale, s_offset);
                         // T = 0 exactly: the FP64 decision is known per time, no guard band
-                        const bool fast_ok = ts.tz ? ts.tz_in : (sidx >= sg_lo && sidx <= sg_hi);
-                        const bool band = act && !fast_ok && !ts.tz && sidx >= sr_lo && sidx <= sr_hi;
+                        const float x = fabsf(sidx - g_mid);
+                        const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
+                        const bool band = act && !fast_ok && !ts.tz && x <= g_out;
                         if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
                         if constexpr (SLOW) {   // re-decide the guard band in FP64
                             ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q],
@@ -713,8 +717,13 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         PSTM_UNROLL(PSTM_UNROLL_PLAIN)
                         for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, F{}, Tr{});
                     }
-                    PSTM_UNROLL(PSTM_UNROLL_TAPER)
-                    for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, Tr{}, F{});
+                    if (small_t) {
+                        PSTM_UNROLL(PSTM_UNROLL_TAPER)
+                        for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, Tr{}, F{});
+                    } else {
+                        PSTM_UNROLL(PSTM_UNROLL_TAPER)
+                        for (int c = n0; c < n; ++c) a += pair(c, Tr{}, F{}, F{}, F{}, F{});
+                    }
                 } else {   // no taper: the aperture edge is a hard cut, ties are decided in FP64
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
                     for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{}, Tr{}, F{});
