@@ -17,8 +17,10 @@
 //            traveltime, sample index, linear interpolation (from shared
 //            memory) and weights, with warp-uniform skips instead of
 //            divergent branches.
-// Chunk partials are folded into compensated (TwoSum) FP32 sums and the
-// epilogue adds them once into the caller's image (+=) and fold.
+// Chunk partials are added into FP32 partial sums in shared memory (with
+// their TwoSum rounding errors kept apart when compensated accumulation is
+// on), which are added into the caller's image (+=) every 16 chunks and at
+// the end; the fold is added in the epilogue.
 //
 // Reference semantics (paths relative to the reference project):
 //   loop structure, fold, aperture, taper, weights  numba_cpu_optimized.py:147-231
@@ -361,7 +363,10 @@ __host__ __device__ constexpr int record_buffer_bytes(int PB, bool has_c) {
 }
 __host__ __device__ constexpr int geo_buffer_bytes() { return kMaxChunk * kGeoDoubles * 8; }
 // Per-lane FP32 partial sums of one CTA: PB x R x kThreads floats.
-__host__ __device__ constexpr int partial_bytes(int PB, int R) { return PB * R * kThreads * 4; }
+// FP32 partial sums of a CTA, and with compensated accumulation their TwoSum error terms.
+__host__ __device__ constexpr int partial_bytes(int PB, int R, bool compensated = false) {
+    return PB * R * kThreads * 4 * (compensated ? 2 : 1);
+}
 
 // ---------------------------------------------------------------- the kernel
 // What one work item migrates: PB pillars x one block of 512*R output times of
@@ -411,6 +416,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     unsigned char *const geo_base = smem + 2 * amp_bytes;
     unsigned char *const rec_base = geo_base + 2 * geo_buffer_bytes();
     float *const s_acc = reinterpret_cast<float *>(rec_base + 2 * REC_BYTES);   // [PB][R][kThreads]
+    const bool comp = P.compensated != 0;
+    float *const s_err = s_acc + PB * R * kThreads;   // [PB][R][kThreads] when comp
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pbx = it.pbx, pby = it.pby;
@@ -444,7 +451,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     const int64_t n_chunks = (it.n_traces + C - 1) / C;
     const int flush_every = P.flush_every;
 
-    for (int i = tid; i < PB * R * kThreads; i += kThreads) s_acc[i] = 0.f;
+    for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
 
     // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
     // rows when they are 16-byte aligned) into buffer b
@@ -562,7 +569,13 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
 #pragma unroll 1
             for (int r = 0; r < R; ++r) {
                 const int t = t_lane + r * kThreads;
-                float &a = s_acc[(q * R + r) * kThreads + tid];
+                float &sa = s_acc[(q * R + r) * kThreads + tid];
+                float a = sa;
+                if (comp) {   // the partial and its rounding error, summed in FP32 once more
+                    float &se = s_err[(q * R + r) * kThreads + tid];
+                    a += se;
+                    se = 0.f;
+                }
                 if (p >= 0 && t < P.nt && a != 0.f) {
                     const int64_t idx = (int64_t)p * P.nt + t;
                     if (P.atomic_flush) {   // items of several trace segments share the outputs
@@ -574,7 +587,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         reinterpret_cast<double *>(it.image)[idx] += (double)a;
                     }
                 }
-                a = 0.f;
+                sa = 0.f;
             }
         }
     };
@@ -736,7 +749,14 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         a += pair(c, Tr{}, Tr{}, Tr{}, Tr{}, F{});
                     }
                 }
-                s_acc[(q * R + r) * kThreads + tid] += a;
+                float &sa = s_acc[(q * R + r) * kThreads + tid];
+                if (comp) {   // TwoSum: sa + a = t + e exactly; the errors are kept apart
+                    const float s0 = sa, t = s0 + a, bp = t - s0;
+                    s_err[(q * R + r) * kThreads + tid] += (s0 - (t - bp)) + (a - bp);
+                    sa = t;
+                } else {
+                    sa += a;
+                }
             }
         }
 

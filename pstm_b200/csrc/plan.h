@@ -165,7 +165,7 @@ inline bool plan_staging(KParams &P, const pstm_traces_desc *tr, const pstm_para
     P.bulk = (aligned && tr->amp_row_stride >= pitch) ? 1 : 0;
     const bool has_c = prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI;
     const size_t fixed = 2 * (size_t)geo_buffer_bytes() + 2 * (size_t)record_buffer_bytes(PB, has_c) +
-                         (size_t)partial_bytes(PB, R);
+                         (size_t)partial_bytes(PB, R, prm->compensated != 0);
     const size_t static_bytes = 3072;   // s_ox/s_oy/s_pid/s_fold/s_rank/barriers, rounded up
     const size_t budget = (size_t)smem_optin > fixed + static_bytes ? smem_optin - fixed - static_bytes : 0;
     int chunk = (int)(budget / (2 * (size_t)pitch * eb));

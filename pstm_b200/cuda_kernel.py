@@ -68,7 +68,9 @@ class CudaKernel:
         arrays as BF16 bit patterns; ``"bf16"``/``"f16"``/``"f32"`` convert on
         the host first (the precision form stores traces in 16 bits).
     compensated:
-        Compensated (TwoSum) FP32 accumulation across trace chunks.
+        TwoSum-compensated FP32 partial sums between the flushes into the
+        image (``True``/``False``); ``"auto"`` compensates for 16-bit traces
+        (the precision form) and not for FP32 traces.
     velocity_mode:
         ``"exact"`` uses a 3-D velocity slice per pillar; ``"auto"`` follows the
         Metal host rule (``metal_compiled.py:631-664``): the centre pillar is
@@ -80,10 +82,12 @@ class CudaKernel:
     """
 
     def __init__(self, device: int | None = None, trace_dtype: str = "auto",
-                 compensated: bool = True, velocity_mode: str = "exact", precision: str = "exact"):
+                 compensated="auto", velocity_mode: str = "exact", precision: str = "exact"):
         self._device = int(os.environ.get("PSTM_CUDA_DEVICE", "0")) if device is None else int(device)
         self._trace_dtype = trace_dtype
-        self._compensated = bool(compensated)
+        if compensated not in ("auto", True, False):
+            raise ValueError("compensated must be 'auto', True or False")
+        self._compensated = compensated
         self._velocity_mode = velocity_mode
         if precision not in ("exact", "fast"):
             raise ValueError("precision must be 'exact' or 'fast'")
@@ -215,6 +219,7 @@ class CudaKernel:
         vd.vrms, vd.is_3d, dv = self._velocity(velocity, output, od.nx, od.ny, od.nt, keep)
         devs.append(dv)
         prm = self._params(cfg, _TT_BY_TYPE[kernel_type], keep, devs=devs)
+        self._auto_compensation(prm, td)
         if not all(devs):
             raise ValueError("the learned form takes CUDA tensors only")
         net = surrogate.to_struct()
@@ -277,7 +282,7 @@ class CudaKernel:
         p.curved_v0 = float(getattr(cfg, "curved_ray_v0", 1500.0))
         p.curved_k = float(getattr(cfg, "curved_ray_k", 0.5))
         p.eta_constant = float(getattr(cfg, "vti_eta_constant", 0.0))
-        p.compensated = int(self._compensated)
+        p.compensated = 0 if self._compensated == "auto" else int(bool(self._compensated))
         p.precision = self._precision
         p.interpolation = nat.interp_code(getattr(cfg, "interpolation_method", None))
         eta = eta_override if eta_override is not None else getattr(cfg, "vti_eta_array", None)
@@ -288,6 +293,12 @@ class CudaKernel:
             p.eta = ptr
             p.eta_is_3d = 0 if len(eta.shape) == 1 else 1
         return p
+
+    def _auto_compensation(self, prm, td) -> None:
+        """compensated="auto": TwoSum-compensated partial sums for 16-bit traces
+        (the precision form), plain FP32 partials for FP32 traces."""
+        if self._compensated == "auto":
+            prm.compensated = int(td.amp_dtype != nat.AMP_F32)
 
     def _arr(self, a, dtype, keep: list):
         """(pointer, on_device) for a numpy array or a CUDA torch tensor."""
@@ -446,6 +457,7 @@ class CudaKernel:
         vd.vrms, vd.is_3d, dv = self._velocity(velocity, output, nx, ny, nt, keep)
         devs.append(dv)
         prm = self._params(cfg, tt, keep, devs=devs)
+        self._auto_compensation(prm, td)
 
         on_dev = all(devs)
         if any(devs) and not on_dev:
@@ -494,6 +506,7 @@ def _batch_descs(kernel: "CudaKernel", traces, bins, geometry, velocity, config,
     vd.vrms, vd.is_3d, dv = kernel._velocity(velocity, geometry, nx, ny, nt, keep)
     devs.append(dv)
     prm = kernel._params(cfg, _TT_BY_TYPE[kernel_type], keep, devs=devs)
+    kernel._auto_compensation(prm, td)
     if not all(devs):
         raise ValueError("the batched form takes CUDA tensors only (traces, axes, velocity and eta)")
     arr = (nat.BinDesc * max(1, len(bins)))()

@@ -237,3 +237,21 @@ def test_invalid_arguments_and_injected_fault(cuda_kernel_factory, monkeypatch):
     k.migrate_tile(case.traces, case.output, case.velocity)   # context still usable
     ref = oracle_run(case.traces, case.output, case.velocity, case.config)
     assert rel_l2(case.output.image, ref.image) <= PLAIN_TOL
+
+
+def test_compensated_partials(cuda_kernel_factory):
+    """TwoSum-compensated partial sums (the precision form's accumulation) stay
+    within the plain tolerance and no farther from the FP64 oracle than the
+    plain FP32 partials."""
+    from pstm_b200 import workloads
+    case = workloads.config1(n_traces=4000, nx=8, ny=6, nt=500)
+    out = case.output
+    ref = oracle_run(case.traces, out, case.velocity, case.config)
+    errs = {}
+    for comp in (False, True):
+        k = cuda_kernel_factory(case.config, compensated=comp)
+        o = fresh(out)
+        k.migrate_tile(case.traces, o, case.velocity)
+        np.testing.assert_array_equal(o.fold, ref.fold)
+        errs[comp] = rel_l2(o.image, ref.image)
+    assert errs[True] <= PLAIN_TOL and errs[True] <= errs[False] * 1.05 + 1e-9, errs
