@@ -9,9 +9,15 @@
 // the tiled gather kernel; the other methods run here, in FP64 (traveltime,
 // sample index, interpolation weights and accumulation), with one CTA of 128
 // threads per (pillar, block of 128 output times) and the traces read from
-// the packed geometry and the caller's panel.  Aperture, taper, weights, AA
-// and fold are those of the gather kernel.
+// the packed geometry and the caller's panel.  The CTA stages the traces 128
+// at a time: each thread takes one trace's pillar distances, counts it for the
+// fold and keeps it if it lies inside the largest aperture of the CTA's times;
+// the kept traces, in trace order, go to shared memory and every thread then
+// runs them against its own output time.  Aperture, taper, weights, AA and
+// fold are those of the gather kernel.
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 #include "pstm_cuda.h"
 #include "kparams.h"
@@ -24,31 +30,23 @@ using namespace pstm::ctx;
 
 namespace {
 
+constexpr int kInterpThreads = 128;
+
 template <int AMP>
 __device__ inline double sample_at(const unsigned char *row, int64_t i) {
     return (double)amp_at<AMP>(row, (int)i);
 }
 
-__device__ inline double sinc_pi(double x) { return fabs(x) < 1e-10 ? 1.0 : sinpi(x) / (M_PI * x); }
-
-// One interpolated sample at fractional index t (0 <= t < ns - 1 is checked by the caller).
+// Nearest, Catmull-Rom cubic and linear interpolation at fractional index t
+// (0 <= t < ns - 1 is checked by the caller); linear also serves the wide
+// methods within their half-width of a trace end.
 template <int AMP>
-__device__ double interpolate(const unsigned char *row, int ns, double t, int method) {
+__device__ double interpolate_narrow(const unsigned char *row, int ns, double t, int method) {
     if (method == PSTM_INTERP_NEAREST) {
         const int64_t i = (int64_t)(t + 0.5);
         return (i < 0 || i >= ns) ? 0.0 : sample_at<AMP>(row, i);
     }
-    const int hw = method == PSTM_INTERP_SINC4 ? 2 : method == PSTM_INTERP_SINC8 ? 4
-                 : method == PSTM_INTERP_SINC16 ? 8 : method == PSTM_INTERP_LANCZOS3 ? 3
-                 : method == PSTM_INTERP_LANCZOS5 ? 5 : 0;
-    const bool cubic_edge = method == PSTM_INTERP_CUBIC && (t < 1.0 || t >= (double)(ns - 2));
-    const bool wide_edge = hw > 0 && (t < (double)hw || t >= (double)(ns - hw));
-    if (method == PSTM_INTERP_LINEAR || cubic_edge || wide_edge || (method != PSTM_INTERP_CUBIC && hw == 0)) {
-        const int64_t i0 = (int64_t)t;
-        const double f = t - (double)i0;
-        return sample_at<AMP>(row, i0) * (1.0 - f) + sample_at<AMP>(row, i0 + 1) * f;
-    }
-    if (method == PSTM_INTERP_CUBIC) {   // Catmull-Rom
+    if (method == PSTM_INTERP_CUBIC && t >= 1.0 && t < (double)(ns - 2)) {   // Catmull-Rom
         const int64_t i = (int64_t)t;
         const double u = t - (double)i;
         const double p0 = sample_at<AMP>(row, i - 1), p1 = sample_at<AMP>(row, i);
@@ -58,19 +56,78 @@ __device__ double interpolate(const unsigned char *row, int ns, double t, int me
         const double c1 = -0.5 * p0 + 0.5 * p2;
         return ((c3 * u + c2) * u + c1) * u + p1;
     }
-    const bool lanczos = method == PSTM_INTERP_LANCZOS3 || method == PSTM_INTERP_LANCZOS5;
-    const int64_t ic = lanczos ? (int64_t)t : (int64_t)(t + 0.5);
+    const int64_t i0 = (int64_t)t;
+    const double f = t - (double)i0;
+    return sample_at<AMP>(row, i0) * (1.0 - f) + sample_at<AMP>(row, i0 + 1) * f;
+}
+
+// Windowed sinc (LANCZOS false) or Lanczos (true) of half-width HW at
+// fractional index t, normalised by the sum of the weights; linear within HW
+// samples of a trace end.
+//
+// The taps need sin(pi x) and the sine or cosine of pi x / HW at x = frac - k,
+// k = -HW+1 .. HW.  Since sin(pi (frac - k)) = (-1)^k sin(pi frac) and the
+// window angle pi (frac - k) / HW moves by pi / HW from one tap to the next,
+// one sincospi of frac and a chain of window angles carried by rotations
+// through (cos_d, sin_d) = (cos, sin)(pi / HW) give every weight.  A rotation
+// adds about one rounding of a unit-sized value per tap (absolute 1e-15 after
+// 16 taps), harmless where the window enters as 0.5 (1 + cos).  Lanczos
+// divides sin(pi x / HW) by x, so it needs that sine accurate relative to its
+// size near x = 0: it runs two chains, each started by its own sincospi at a
+// tap beside x = 0 (k = 0 and k = 1) and carried outward.  The weights are
+// otherwise those of the direct formulas: sinc(x) = sin(pi x) / (pi x) with 1
+// for |x| < 1e-10, a Hann window 0.5 (1 + cos(pi x / HW)) that is 0 for
+// |x| >= HW, Lanczos sinc(x) sinc(x / HW).
+template <int AMP, int HW, bool LANCZOS>
+__device__ double interpolate_wide(const unsigned char *row, int ns, double t, double cos_d, double sin_d) {
+    if (t < (double)HW || t >= (double)(ns - HW)) {
+        const int64_t i0 = (int64_t)t;
+        const double f = t - (double)i0;
+        return sample_at<AMP>(row, i0) * (1.0 - f) + sample_at<AMP>(row, i0 + 1) * f;
+    }
+    const int64_t ic = LANCZOS ? (int64_t)t : (int64_t)(t + 0.5);
     const double frac = t - (double)ic;
+    double s_f, c_f;
+    sincospi(frac, &s_f, &c_f);
     double acc = 0.0, norm = 0.0;
-    for (int k = -hw + 1; k <= hw; ++k) {
+    auto tap = [&](int k, double s_k, double s_w, double c_w) {
         const int64_t i = ic + k;
-        if (i < 0 || i >= ns) continue;   // (sinc rounds to the nearest sample: ic + hw can reach ns)
+        if (i < 0 || i >= ns) return;   // (sinc rounds to the nearest sample: ic + HW can reach ns)
         const double x = frac - (double)k;
         double w;
-        if (lanczos) w = fabs(x) < 1e-10 ? 1.0 : (fabs(x) >= hw ? 0.0 : sinc_pi(x) * sinc_pi(x / hw));
-        else w = sinc_pi(x) * (fabs(x) >= hw ? 0.0 : 0.5 * (1.0 + cospi(x / hw)));
+        if (LANCZOS) w = fabs(x) < 1e-10 ? 1.0 : (fabs(x) >= HW ? 0.0 : (s_k * s_w * HW) / (M_PI * M_PI * x * x));
+        else w = (fabs(x) < 1e-10 ? 1.0 : s_k / (M_PI * x)) * (fabs(x) >= HW ? 0.0 : 0.5 * (1.0 + c_w));
         acc += sample_at<AMP>(row, i) * w;
         norm += w;
+    };
+    if (!LANCZOS) {   // one chain, k = -HW+1 .. HW, window angle dropping by pi / HW per tap
+        double s_w, c_w;
+        sincospi((frac + (double)(HW - 1)) / (double)HW, &s_w, &c_w);
+        double s_k = ((HW - 1) & 1) ? -s_f : s_f;
+#pragma unroll
+        for (int k = -HW + 1; k <= HW; ++k) {
+            tap(k, s_k, s_w, c_w);
+            const double c_n = c_w * cos_d + s_w * sin_d;
+            s_w = s_w * cos_d - c_w * sin_d;
+            c_w = c_n;
+            s_k = -s_k;
+        }
+    } else {          // k = 0, -1, .., -HW+1 (angle growing), then k = 1, .., HW (angle dropping)
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const double sin_a = side ? -sin_d : sin_d;
+            double s_w, c_w;
+            sincospi((frac - (double)side) / (double)HW, &s_w, &c_w);
+            double s_k = side ? -s_f : s_f;
+#pragma unroll
+            for (int n = 0; n < HW; ++n) {
+                tap(side ? 1 + n : -n, s_k, s_w, c_w);
+                const double c_n = c_w * cos_d - s_w * sin_a;
+                s_w = s_w * cos_d + c_w * sin_a;
+                c_w = c_n;
+                s_k = -s_k;
+            }
+        }
     }
     return norm > 1e-10 ? acc / norm : 0.0;
 }
@@ -80,12 +137,23 @@ __device__ inline double tt_of(double t0, double ds2, double dr2, double v, doub
     return traveltime_fp64<TT>(t0, ds2, dr2, v, eta, v0, k);
 }
 
-template <int AMP>
-__global__ void __launch_bounds__(128) migrate_interp_kernel(const KParams P, int tt, int method) {
+// Per-trace values staged in shared memory for the CTA's pillar.
+struct Staged {
+    double ds2[kInterpThreads], dr2[kInterpThreads], d[kInterpThreads], w[kInterpThreads], m[kInterpThreads];
+    int tr[kInterpThreads];
+    int kept[kInterpThreads / 32];
+    int fold[kInterpThreads / 32];
+    double ap[kInterpThreads / 32];
+};
+
+template <int AMP, int HW, bool LANCZOS>
+__global__ void __launch_bounds__(kInterpThreads) migrate_interp_kernel(const KParams P, int tt, int method) {
+    __shared__ Staged S;
     const int p = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ix = p / P.ny, iy = p - ix * P.ny;
     const double ox = P.xg ? P.xg[p] : P.xa[ix], oy = P.yg ? P.yg[p] : P.ya[iy];
-    const int t = blockIdx.y * blockDim.x + threadIdx.x;
+    const int t = blockIdx.y * kInterpThreads + threadIdx.x;
     const bool tv = t < P.nt;
     const int tc = tv ? t : P.nt - 1;
     const double t0 = P.ta[tc] / 1000.0;
@@ -100,45 +168,90 @@ __global__ void __launch_bounds__(128) migrate_interp_kernel(const KParams P, in
         vw = P.cr_v0 + P.cr_k * z;
     }
     const double gmax = P.aa_gmax, fdom = P.aa_fdom;
+    const double inv_vw = 1.0 / vw;
     const double taper_start = ap * (1.0 - P.taper);
+    double sin_d = 0.0, cos_d = 1.0;
+    if (HW > 0) sincospi(1.0 / (double)HW, &sin_d, &cos_d);
+
+    // Largest aperture over the CTA's output times: a trace farther than it
+    // from the pillar adds nothing at any of them.
+    double ap_cta = tv ? ap : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ap_cta = fmax(ap_cta, __shfl_xor_sync(0xffffffffu, ap_cta, o));
+    if (lane == 0) { S.ap[warp] = ap_cta; S.fold[warp] = 0; }
+    __syncthreads();
+    ap_cta = fmax(fmax(S.ap[0], S.ap[1]), fmax(S.ap[2], S.ap[3]));
+
     double acc = 0.0;
-    int cnt = 0;
-    for (int64_t tr = 0; tr < P.n_traces; ++tr) {
+    for (int64_t c0 = 0; c0 < P.n_traces; c0 += kInterpThreads) {
+        const int64_t tr = c0 + threadIdx.x;
+        bool keep = false, in_fold = false;
+        double dxm = 0.0, dym = 0.0, d = 0.0;
         const double *g = P.geo + tr * kGeoDoubles;
-        const double dxm = ox - g[4], dym = oy - g[5];
-        const double d2 = dxm * dxm + dym * dym;
-        cnt += d2 <= P.fold_d2_max;
-        const double d = sqrt(d2);
-        const bool act = tv && !(d > ap);
-        if (!__any_sync(0xffffffffu, act)) continue;
-        if (!act) continue;
-        const double dxs = ox - g[0], dys = oy - g[1], dxr = ox - g[2], dyr = oy - g[3];
-        const double ds2 = dxs * dxs + dys * dys, dr2 = dxr * dxr + dyr * dyr;
-        double T;
-        switch (tt) {
-        case TT_CURVED: T = tt_of<TT_CURVED>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
-        case TT_VTI: T = tt_of<TT_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
-        case TT_CURVED_VTI: T = tt_of<TT_CURVED_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
-        default: T = tt_of<TT_STRAIGHT>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
+        if (tr < P.n_traces) {
+            dxm = ox - g[4];
+            dym = oy - g[5];
+            const double d2 = dxm * dxm + dym * dym;
+            in_fold = d2 <= P.fold_d2_max;
+            d = sqrt(d2);
+            keep = !(d > ap_cta);
         }
-        const double s = (T - P.tstart_s) / P.dt_s;
-        if (!(s >= 0.0 && s < (double)(P.ns - 1))) continue;
-        const unsigned char *row =
-            reinterpret_cast<const unsigned char *>(P.amps) + (tr * P.amp_stride) * (int64_t)P.elem;
-        const double amp = interpolate<AMP>(row, P.ns, s, method);
-        double w = g[6];
-        if (d > taper_start) w *= 0.5 * (1.0 + cospi((d - taper_start) / (ap - taper_start)));
-        if (P.aa && T >= 0.001) {
-            const double st = fmin(fmax(fabs(dxm), fabs(dym)) / (vw * T), 1.0);
-            if (st >= 0.01) {
-                const double fmx = fmin(vw / (4.0 * gmax * st), 500.0);
-                w *= fmax(0.0, 1.0 - fdom / fmx);
+        const unsigned kb = __ballot_sync(0xffffffffu, keep), fb = __ballot_sync(0xffffffffu, in_fold);
+        if (lane == 0) { S.kept[warp] = __popc(kb); S.fold[warp] += __popc(fb); }
+        __syncthreads();
+        int base = 0, n_kept = 0;
+#pragma unroll
+        for (int w = 0; w < kInterpThreads / 32; ++w) {
+            base += w < warp ? S.kept[w] : 0;
+            n_kept += S.kept[w];
+        }
+        if (keep) {
+            const int j = base + __popc(kb & ((1u << lane) - 1u));
+            const double dxs = ox - g[0], dys = oy - g[1], dxr = ox - g[2], dyr = oy - g[3];
+            S.ds2[j] = dxs * dxs + dys * dys;
+            S.dr2[j] = dxr * dxr + dyr * dyr;
+            S.d[j] = d;
+            S.w[j] = g[6];
+            S.m[j] = fmax(fabs(dxm), fabs(dym));
+            S.tr[j] = (int)tr;
+        }
+        __syncthreads();
+        for (int j = 0; j < n_kept; ++j) {
+            const double dj = S.d[j];
+            if (!tv || dj > ap) continue;
+            const double ds2 = S.ds2[j], dr2 = S.dr2[j];
+            double T;
+            switch (tt) {
+            case TT_CURVED: T = tt_of<TT_CURVED>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
+            case TT_VTI: T = tt_of<TT_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
+            case TT_CURVED_VTI: T = tt_of<TT_CURVED_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
+            default: T = tt_of<TT_STRAIGHT>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
             }
+            const double s = (T - P.tstart_s) / P.dt_s;
+            if (!(s >= 0.0 && s < (double)(P.ns - 1))) continue;
+            const unsigned char *row =
+                reinterpret_cast<const unsigned char *>(P.amps) + ((int64_t)S.tr[j] * P.amp_stride) * (int64_t)P.elem;
+            double amp;
+            if (HW > 0) amp = interpolate_wide<AMP, HW, LANCZOS>(row, P.ns, s, cos_d, sin_d);
+            else amp = interpolate_narrow<AMP>(row, P.ns, s, method);
+            double w = S.w[j];
+            if (dj > taper_start) w *= 0.5 * (1.0 + cospi((dj - taper_start) / (ap - taper_start)));
+            // One reciprocal of T per pair and 1/v per thread serve the AA,
+            // spreading and obliquity terms: sin = m / (v T), f_max = min(v /
+            // (4 gmax sin), 500 Hz) so f_dom / f_max = f_dom max(4 gmax sin / v,
+            // 1 / 500), spreading 1 / (v T), obliquity t0 / T.
+            const double inv_T = 1.0 / T;
+            if (P.aa && T >= 0.001) {
+                const double st = fmin(S.m[j] * inv_T * inv_vw, 1.0);
+                if (st >= 0.01) w *= fmax(0.0, 1.0 - fdom * fmax(4.0 * gmax * st * inv_vw, 1.0 / 500.0));
+            }
+            if (P.spreading && T > 0.001) w *= inv_T * inv_vw;
+            if (P.obliquity && T > 0.001) w *= t0 * inv_T;
+            acc += amp * w;
         }
-        if (P.spreading && T > 0.001) w *= 1.0 / (vw * T);
-        if (P.obliquity && T > 0.001) w *= t0 / T;
-        acc += amp * w;
+        __syncthreads();   // the next batch overwrites the staged values
     }
+    const int cnt = S.fold[0] + S.fold[1] + S.fold[2] + S.fold[3];
     if (tv) {
         const int64_t idx = (int64_t)p * P.nt + t;
         if (P.image_f32) reinterpret_cast<float *>(P.image)[idx] += (float)acc;
@@ -148,17 +261,35 @@ __global__ void __launch_bounds__(128) migrate_interp_kernel(const KParams P, in
     if (P.fold && !P.fold3d && blockIdx.y == 0 && threadIdx.x == 0) P.fold[p] += cnt;
 }
 
+template <int AMP, int HW, bool LANCZOS>
+void launch_one(const TilePlan &tp, dim3 grid, int method) {
+    migrate_interp_kernel<AMP, HW, LANCZOS><<<grid, kInterpThreads, 0, tp.L.stream>>>(tp.P, tp.tt, method);
+}
+
+template <int AMP>
+void launch_method(const TilePlan &tp, dim3 grid, int method) {
+    switch (method) {
+    case PSTM_INTERP_SINC4: launch_one<AMP, 2, false>(tp, grid, method); break;
+    case PSTM_INTERP_SINC8: launch_one<AMP, 4, false>(tp, grid, method); break;
+    case PSTM_INTERP_SINC16: launch_one<AMP, 8, false>(tp, grid, method); break;
+    case PSTM_INTERP_LANCZOS3: launch_one<AMP, 3, true>(tp, grid, method); break;
+    case PSTM_INTERP_LANCZOS5: launch_one<AMP, 5, true>(tp, grid, method); break;
+    default: launch_one<AMP, 0, false>(tp, grid, method); break;   // nearest, cubic, linear
+    }
+}
+
 }  // namespace
 
 namespace pstm {
 namespace ctx {
 // Launch of the higher-order-interpolation kernel on a prepared tile.
 int32_t launch_interp(Ctx *c, const TilePlan &tp, int method, const pstm_output_desc *out) {
-    const dim3 grid((unsigned)((int64_t)out->nx * out->ny), (unsigned)((out->nt + 127) / 128));
+    if (tp.P.n_traces > INT32_MAX) return fail(c, PSTM_ERR_INVALID_ARGUMENT, "interpolation kernel takes at most 2^31 - 1 traces");
+    const dim3 grid((unsigned)((int64_t)out->nx * out->ny), (unsigned)((out->nt + kInterpThreads - 1) / kInterpThreads));
     switch (tp.amp) {
-    case PSTM_AMP_F32: migrate_interp_kernel<AMP_F32><<<grid, 128, 0, tp.L.stream>>>(tp.P, tp.tt, method); break;
-    case PSTM_AMP_BF16: migrate_interp_kernel<AMP_BF16><<<grid, 128, 0, tp.L.stream>>>(tp.P, tp.tt, method); break;
-    default: migrate_interp_kernel<AMP_F16><<<grid, 128, 0, tp.L.stream>>>(tp.P, tp.tt, method); break;
+    case PSTM_AMP_F32: launch_method<AMP_F32>(tp, grid, method); break;
+    case PSTM_AMP_BF16: launch_method<AMP_BF16>(tp, grid, method); break;
+    default: launch_method<AMP_F16>(tp, grid, method); break;
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "interpolation migrate kernel launch");
