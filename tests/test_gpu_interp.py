@@ -71,3 +71,34 @@ def test_unknown_method_and_linear_only_forms(cuda_kernel_factory):
     with pytest.raises(ValueError, match="interpolation"):
         k.migrate_tile(case.traces, case.output, case.velocity,
                        dataclasses.replace(case.config, interpolation_method="bicubic-ish"))
+
+
+@pytest.mark.parametrize("method", ["cubic", "sinc8", "lanczos3"])
+def test_bf16_traces_rotated_grid_f32_image_2d_fold(method, cuda_kernel_factory):
+    """BF16 traces, an FP32 image with a 2-D fold on a rotated grid, a trace count
+    that leaves a partial last batch of 128 and an nt that leaves a partial last
+    block of 128 times.  The oracle runs on the BF16-rounded samples; the kernel
+    accumulates in FP64 and rounds once to FP32 (rel L2 <= 1e-6)."""
+    import dataclasses
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile
+    from pstm_b200.cuda_kernel import bf16_bits_to_float32, float32_to_bf16_bits
+    case = workloads.config1(n_traces=333, nx=5, ny=7, nt=300)
+    cfg = dataclasses.replace(case.config, interpolation_method=method, aa_enabled=True)
+    out = case.output
+    X, Y = np.meshgrid(out.x_axis + 300.0, out.y_axis + 200.0, indexing="ij")
+    ang = 0.4
+    Xr = 700 + (X - 700) * np.cos(ang) - (Y - 700) * np.sin(ang)
+    Yr = 700 + (X - 700) * np.sin(ang) + (Y - 700) * np.cos(ang)
+    mk = lambda dt: OutputTile(image=np.zeros(out.image.shape, dt), fold=np.zeros(out.image.shape[:2], np.int32),
+                               x_axis=out.x_axis, y_axis=out.y_axis, t_axis_ms=out.t_axis_ms, x_grid=Xr, y_grid=Yr)
+    got = mk(np.float32)
+    k = cuda_kernel_factory(cfg, trace_dtype="bf16")
+    k.migrate_tile(case.traces, got, case.velocity, cfg)
+    tb = case.traces
+    tq = dataclasses.replace(tb, amplitudes=bf16_bits_to_float32(float32_to_bf16_bits(tb.amplitudes)))
+    ref = mk(np.float64)
+    oracle.migrate(tq, ref, case.velocity, cfg)
+    np.testing.assert_array_equal(got.fold, ref.fold)
+    assert ref.fold.max() > 0 and np.abs(ref.image).max() > 0
+    assert rel_l2(got.image, ref.image) <= 1e-6
