@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define PSTM_CUDA_ABI_VERSION 3
+#define PSTM_CUDA_ABI_VERSION 4
 
 typedef enum {
     PSTM_OK = 0,
@@ -148,6 +148,24 @@ int32_t pstm_cuda_migrate_tile_dev(void *ctx, const pstm_traces_desc *traces,
                                    const pstm_output_desc *output,
                                    const pstm_velocity_desc *velocity,
                                    const pstm_params *params, void *stream);
+
+/* Migrate one tile against the traces of `n_runs` ranges of a resident panel:
+ * runs[2i] .. runs[2i+1] - 1, ascending and disjoint, inside [0, n_traces).
+ * The result is that of pstm_cuda_migrate_tile_dev on the concatenation of the
+ * ranges, up to the order of floating-point additions, without copying the
+ * ranges together: geometry is packed for the span of the runs and one
+ * persistent launch takes (run segment, pillar block, time block) items that
+ * add into the image and fold atomically (non-linear interpolation: one
+ * migration per run).  A panel sorted by midpoint (pstm_b200.spatial) gives
+ * each output tile's traces as a few such runs.  Device pointers;
+ * asynchronous on `stream` as pstm_cuda_migrate_tile_dev.  Replaces the
+ * executor's per-tile trace query and gather, SpatialIndex.query_traces_for_tile
+ * (pstm/data/spatial_index.py:423-460) followed by the trace load of
+ * _process_tile (pstm/pipeline/executor.py:1397-1858). */
+int32_t pstm_cuda_migrate_tile_runs_dev(void *ctx, const pstm_traces_desc *traces, const int64_t *runs,
+                                        int32_t n_runs, const pstm_output_desc *output,
+                                        const pstm_velocity_desc *velocity, const pstm_params *params,
+                                        void *stream);
 
 /* Same, host pointers: inputs are copied to the device, the tile is migrated
  * and image/fold are copied back and accumulated (+=) into the host arrays.

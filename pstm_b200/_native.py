@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpstm_cuda.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # pstm_status
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_INITIALIZED, \
@@ -126,6 +126,9 @@ SIGNATURES = {
     "pstm_cuda_destroy": (None, [_vp]),
     "pstm_cuda_migrate_tile_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                     ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
+    "pstm_cuda_migrate_tile_runs_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(ctypes.c_int64),
+                                                         ctypes.c_int32, ctypes.POINTER(OutputDesc),
+                                                         ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
     "pstm_cuda_migrate_tile_host": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                      ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
     "pstm_cuda_migrate_tile_noalloc": (ctypes.c_int32, [ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "pstm_cuda.h"
@@ -172,6 +173,46 @@ int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc 
     return PSTM_OK;
 }
 
+// Trace-segment length of the segment-major schedule for this tile (0: the
+// context never splits).
+int64_t segment_traces(const Ctx *c, const KParams &P) {
+    if (c->segment_bytes <= 0) return 0;
+    const int64_t row_bytes = (int64_t)P.pitch * P.elem;
+    const int64_t S = c->segment_bytes / row_bytes;
+    return S < 16 * (int64_t)P.chunk ? 16 * (int64_t)P.chunk : S / P.chunk * P.chunk;
+}
+
+// Items for traces [b0, b0 + n) of the prepared panel, S traces at most each
+// (S <= 0: one item).
+void append_segments(std::vector<BinWork> &w, int64_t b0, int64_t n, int64_t S, void *image, int32_t *fold) {
+    if (S <= 0) S = n;
+    for (int64_t b = 0; b < n; b += S) w.push_back({b0 + b, (n - b) < S ? (n - b) : S, image, fold});
+}
+
+// One persistent launch over a list of trace items of the prepared tile, all
+// adding into its image and fold atomically.
+int32_t launch_items(Ctx *c, const TilePlan &tp, const std::vector<BinWork> &w) {
+    if (w.size() > (size_t)0x7fffffff) return fail(c, PSTM_ERR_UNSUPPORTED, "too many trace items for one launch");
+    cudaError_t e;
+    if ((e = ensure(c->seg_bins, w.size() * sizeof(BinWork))) != cudaSuccess ||
+        (e = ensure(c->seg_counter, sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(c, e, "allocating the segment list");
+    if ((e = cudaMemcpyAsync(c->seg_bins.ptr, w.data(), w.size() * sizeof(BinWork), cudaMemcpyHostToDevice,
+                             tp.L.stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->seg_counter.ptr, 0, sizeof(unsigned long long), tp.L.stream)) != cudaSuccess)
+        return cuda_fail(c, e, "writing the segment list");
+    KParams P = tp.P;
+    P.atomic_flush = 1;
+    Launch L;
+    L.smem = tp.L.smem;
+    L.stream = tp.L.stream;
+    L.bins = reinterpret_cast<const BinWork *>(c->seg_bins.ptr);
+    L.n_bins = (int)w.size();
+    L.counter = reinterpret_cast<unsigned long long *>(c->seg_counter.ptr);
+    e = launch_kind(tp.tt, P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, L);
+    return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "segmented migrate kernel launch");
+}
+
 // A panel much larger than L2 is migrated segment by segment: the persistent
 // kernel takes items (trace segment, pillar block, time block) in segment
 // order, so every resident CTA streams the same L2-sized segment at a time
@@ -182,32 +223,9 @@ int32_t launch_tile(Ctx *c, const TilePlan &tp) {
     const KParams &P0 = tp.P;
     const int64_t row_bytes = (int64_t)P0.pitch * P0.elem;
     if (c->segment_bytes > 0 && P0.n_traces * row_bytes > 2 * c->segment_bytes) {
-        int64_t S = c->segment_bytes / row_bytes;
-        S = S < 16 * (int64_t)P0.chunk ? 16 * (int64_t)P0.chunk : S / P0.chunk * P0.chunk;
-        const int64_t nseg = (P0.n_traces + S - 1) / S;
-        std::vector<BinWork> w((size_t)nseg);
-        for (int64_t i = 0; i < nseg; ++i) {
-            const int64_t b = i * S;
-            w[(size_t)i] = {b, (P0.n_traces - b) < S ? (P0.n_traces - b) : S, P0.image, P0.fold};
-        }
-        cudaError_t e;
-        if ((e = ensure(c->seg_bins, w.size() * sizeof(BinWork))) != cudaSuccess ||
-            (e = ensure(c->seg_counter, sizeof(unsigned long long))) != cudaSuccess)
-            return cuda_fail(c, e, "allocating the segment list");
-        if ((e = cudaMemcpyAsync(c->seg_bins.ptr, w.data(), w.size() * sizeof(BinWork), cudaMemcpyHostToDevice,
-                                 tp.L.stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(c->seg_counter.ptr, 0, sizeof(unsigned long long), tp.L.stream)) != cudaSuccess)
-            return cuda_fail(c, e, "writing the segment list");
-        KParams P = P0;
-        P.atomic_flush = 1;
-        Launch L;
-        L.smem = tp.L.smem;
-        L.stream = tp.L.stream;
-        L.bins = reinterpret_cast<const BinWork *>(c->seg_bins.ptr);
-        L.n_bins = (int)nseg;
-        L.counter = reinterpret_cast<unsigned long long *>(c->seg_counter.ptr);
-        e = launch_kind(tp.tt, P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, L);
-        return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "segmented migrate kernel launch");
+        std::vector<BinWork> w;
+        append_segments(w, 0, P0.n_traces, segment_traces(c, P0), P0.image, P0.fold);
+        return launch_items(c, tp, w);
     }
     const cudaError_t e = launch_kind(tp.tt, tp.P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, tp.L);
     return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "migrate kernel launch");
@@ -321,6 +339,67 @@ int32_t pstm_cuda_migrate_tile_dev(void *ctx, const pstm_traces_desc *traces, co
     if (!c) return fail(nullptr, PSTM_ERR_NOT_INITIALIZED, "Kernel not initialized");
     cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->stream;
     return run_dev(c, traces, output, velocity, params, st);
+}
+
+namespace {
+
+// The traces [a, a + n) of a panel as a panel of their own (no copy).
+pstm_traces_desc sub_panel(const pstm_traces_desc &t, int64_t a, int64_t n) {
+    pstm_traces_desc s = t;
+    s.amplitudes = static_cast<const unsigned char *>(t.amplitudes) +
+                   a * t.amp_row_stride * (int64_t)amp_elem_bytes(t.amp_dtype);
+    s.source_x = t.source_x + a;
+    s.source_y = t.source_y + a;
+    s.receiver_x = t.receiver_x + a;
+    s.receiver_y = t.receiver_y + a;
+    s.midpoint_x = t.midpoint_x + a;
+    s.midpoint_y = t.midpoint_y + a;
+    if (t.weights) s.weights = t.weights + a;
+    s.n_traces = n;
+    return s;
+}
+
+}  // namespace
+
+int32_t pstm_cuda_migrate_tile_runs_dev(void *ctx, const pstm_traces_desc *traces, const int64_t *runs,
+                                        int32_t n_runs, const pstm_output_desc *output,
+                                        const pstm_velocity_desc *velocity, const pstm_params *params,
+                                        void *stream) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return fail(nullptr, PSTM_ERR_NOT_INITIALIZED, "Kernel not initialized");
+    if (!traces || n_runs < 0 || (n_runs > 0 && !runs))
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT, "runs: n_runs >= 0 [begin, end) pairs required");
+    int32_t rc = validate(c, traces, output, velocity, params);
+    if (rc) return rc;
+    std::vector<std::pair<int64_t, int64_t>> rv;
+    int64_t prev = 0;
+    for (int32_t i = 0; i < n_runs; ++i) {
+        const int64_t a = runs[2 * i], b = runs[2 * i + 1];
+        if (a < prev || b < a || b > traces->n_traces)
+            return fail(c, PSTM_ERR_INVALID_ARGUMENT,
+                        "runs must be ascending, disjoint [begin, end) trace ranges inside the panel");
+        prev = b;
+        if (b > a) rv.emplace_back(a, b);
+    }
+    if (rv.empty()) return PSTM_OK;   // no traces: image += 0, fold += 0
+    cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->stream;
+    if (params->interpolation != PSTM_INTERP_LINEAR || rv.size() == 1) {
+        for (const auto &r : rv) {
+            const pstm_traces_desc sub = sub_panel(*traces, r.first, r.second - r.first);
+            if ((rc = run_dev(c, &sub, output, velocity, params, st)) != PSTM_OK) return rc;
+        }
+        return PSTM_OK;
+    }
+    // One tile preparation over the span of the runs (geometry packed for the
+    // span) and one persistent launch over the runs' segments.
+    const int64_t a0 = rv.front().first;
+    const pstm_traces_desc span = sub_panel(*traces, a0, rv.back().second - a0);
+    TilePlan tp;
+    if ((rc = prepare_tile(c, &span, output, velocity, params, st, tp)) != PSTM_OK || tp.empty) return rc;
+    const int64_t S = segment_traces(c, tp.P);
+    std::vector<BinWork> w;
+    for (const auto &r : rv) append_segments(w, r.first - a0, r.second - r.first, S, tp.P.image, tp.P.fold);
+    return launch_items(c, tp, w);
 }
 
 static int32_t migrate_host_impl(Ctx *c, const pstm_traces_desc *traces, const pstm_output_desc *output,

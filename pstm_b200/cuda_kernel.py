@@ -410,7 +410,24 @@ class CudaKernel:
             od.y_grid, d5 = self._arr(yg, np.float64, keep)
             devs += [d4, d5]
 
-    def _migrate(self, traces, output, velocity, config, tt: int) -> KernelMetrics:
+    def migrate_tile_runs(self, traces, runs, output, velocity, config=None,
+                          kernel_type: str = "straight_ray") -> KernelMetrics:
+        """Migrate one tile against row ranges of a resident panel.
+
+        ``runs`` is an (n, 2) array of [begin, end) row ranges of ``traces``
+        (CUDA tensors), ascending and disjoint; the tile receives what
+        ``migrate_tile`` would add for the concatenation of the ranges (up to
+        the order of floating-point additions), without copying them together.
+        A panel in midpoint order (``pstm_b200.spatial``) gives a tile's
+        traces as such ranges.  ``kernel_type`` picks the traveltime as the
+        executor's dispatch does (``executor.py:1691-1745``).
+        """
+        if kernel_type not in _TT_BY_TYPE:
+            raise ValueError(f"unknown kernel_type {kernel_type!r}")
+        r = np.ascontiguousarray(np.asarray(runs, dtype=np.int64).reshape(-1, 2))
+        return self._migrate(traces, output, velocity, config, _TT_BY_TYPE[kernel_type], runs=r)
+
+    def _migrate(self, traces, output, velocity, config, tt: int, runs=None) -> KernelMetrics:
         if self._ctx is None or self._config is None:
             raise RuntimeError("Kernel not initialized")
         cfg = config if config is not None else self._config
@@ -462,6 +479,17 @@ class CudaKernel:
         on_dev = all(devs)
         if any(devs) and not on_dev:
             raise ValueError("mixing device tensors and host arrays in one call is not supported")
+        if runs is not None:
+            if not on_dev:
+                raise ValueError("migrate_tile_runs takes CUDA tensors only")
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+            rc = self._lib.pstm_cuda_migrate_tile_runs_dev(
+                self._ctx, ctypes.byref(td), runs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(runs),
+                ctypes.byref(od), ctypes.byref(vd), ctypes.byref(prm), ctypes.c_void_p(stream))
+            nat.check(rc, self._ctx, self._lib)
+            return KernelMetrics(n_traces_processed=int((runs[:, 1] - runs[:, 0]).sum()) if len(runs) else 0,
+                                 n_samples_output=nx * ny * nt, compute_time_s=time.perf_counter() - t_start)
         if on_dev:
             import torch   # order the launch after the producers of the caller's tensors
             stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY

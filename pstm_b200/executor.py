@@ -12,7 +12,13 @@ other trace is outside the aperture of every pillar of the tile, so it adds
 nothing to the image or the fold), they are gathered into a contiguous tile
 panel, migrated by ``CudaKernel`` and the tile is added into the full image.
 
-Torch holds the buffers and does the selection/gather plumbing.
+With ``spatial`` the executor first puts the panel in midpoint order
+(``pstm_b200.spatial``): a tile's selection box is then a few contiguous row
+ranges found by binary search, and the tile is migrated against them in place
+(``CudaKernel.migrate_tile_runs``), with no per-tile gather.  The learned form
+keeps the gather (its probe and fallback decide per gathered tile).
+
+Torch holds the buffers and does the remaining selection/gather plumbing.
 """
 from __future__ import annotations
 
@@ -42,6 +48,7 @@ class TileResult:
     n_traces: int
     pairs: int          # pillars x samples x selected traces
     kernel_ms: float    # CUDA-event time of the migration call
+    processed_traces: int | None = None   # rows the kernel read (spatial mode: whole runs)
     used_surrogate: bool | None = None
     probe_max_ms: float | None = None
 
@@ -52,12 +59,15 @@ class TiledExecutor:
     ``traces`` is a TraceBlock of CUDA tensors holding the whole survey;
     ``velocity(ix0, ix1, iy0, iy1)`` returns the tile's v_rms as a CUDA tensor
     (nt,) or (tile_nx, tile_ny, nt); ``x_axis``/``y_axis``/``t_axis_ms`` are the
-    full grid's axes (NumPy).
+    full grid's axes (NumPy).  ``spatial`` (True, or a column width in m;
+    True takes an eighth of a tile's width) sorts the panel into midpoint order
+    once -- a second copy of the panel while the caller holds the first -- and
+    migrates each tile against its row ranges in place.
     """
 
     def __init__(self, kernel, traces, x_axis, y_axis, t_axis_ms, velocity, config,
                  kernel_type: str = "straight_ray", tile: int = 64, surrogate=None,
-                 max_residual_ms: float = 0.1):
+                 max_residual_ms: float = 0.1, spatial: bool | float = False):
         import torch
         self.torch = torch
         self.k = kernel
@@ -72,6 +82,17 @@ class TiledExecutor:
         self.max_residual_ms = max_residual_ms
         dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
         self._x, self._y, self._t = dev(self.x_axis), dev(self.y_axis), dev(self.t_axis_ms)
+        self.index = None
+        if spatial is not False and spatial is not None:
+            from .spatial import MidpointIndex, sort_panel
+            if spatial is True:
+                dx = abs(float(self.x_axis[1] - self.x_axis[0])) if len(self.x_axis) > 1 else 1.0
+                width = max(self.tile * dx / 8.0, 1e-3)
+            else:
+                width = float(spatial)
+            host = lambda a: a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+            self.index = MidpointIndex(host(traces.midpoint_x), host(traces.midpoint_y), width)
+            self.tb = sort_panel(traces, self.index)
 
     def tiles(self):
         return tile_ranges(len(self.x_axis), len(self.y_axis), self.tile)
@@ -79,6 +100,8 @@ class TiledExecutor:
     def select(self, tile):
         """Indices (CUDA int64, ascending) of the traces that can reach the tile."""
         x_lo, x_hi, y_lo, y_hi = selection_box(self.x_axis, self.y_axis, tile, self.cfg.max_aperture_m)
+        if self.index is not None:
+            return self.torch.as_tensor(self.index.select(x_lo, x_hi, y_lo, y_hi), device="cuda")
         mx, my = self.tb.midpoint_x, self.tb.midpoint_y
         m = (mx >= x_lo) & (mx <= x_hi) & (my >= y_lo) & (my <= y_hi)
         return self.torch.nonzero(m).squeeze(1)
@@ -99,13 +122,19 @@ class TiledExecutor:
         torch = self.torch
         from .base import OutputTile
         ix0, ix1, iy0, iy1 = tile
-        idx = self.select(tile)
-        n = int(idx.numel())
         nt = len(self.t_axis_ms)
-        res = TileResult(tile, n, (ix1 - ix0) * (iy1 - iy0) * nt * n, 0.0)
-        if n == 0:
+        runs = None
+        if self.index is not None and self.surrogate is None:
+            runs, n = self.index.runs(*selection_box(self.x_axis, self.y_axis, tile, self.cfg.max_aperture_m),
+                                      with_count=True)
+            processed = int((runs[:, 1] - runs[:, 0]).sum()) if len(runs) else 0
+        else:
+            idx = self.select(tile)
+            n = processed = int(idx.numel())
+        res = TileResult(tile, n, (ix1 - ix0) * (iy1 - iy0) * nt * n, 0.0, processed_traces=processed)
+        if processed == 0:
             return res
-        sub = self._gather(idx)
+        sub = self._gather(idx) if runs is None else None
         timg = torch.zeros((ix1 - ix0, iy1 - iy0, nt), dtype=image.dtype, device="cuda")
         tfold = None
         if fold is not None:
@@ -119,6 +148,8 @@ class TiledExecutor:
             _, rep = self.k.migrate_tile_learned(sub, out, vel, self.surrogate, self.cfg, kernel_type=self.kind,
                                                  max_residual_ms=self.max_residual_ms)
             res.used_surrogate, res.probe_max_ms = rep["used_surrogate"], rep["probe_max_ms"]
+        elif runs is not None:
+            self.k.migrate_tile_runs(self.tb, runs, out, vel, self.cfg, kernel_type=self.kind)
         else:
             method = {"straight_ray": self.k.migrate_tile, "curved_ray": self.k.migrate_tile_curved_ray,
                       "anisotropic_vti": self.k.migrate_tile_vti,
