@@ -318,7 +318,7 @@ int pstm_oracle_migrate(const oracle_args *a)
 
 /*
  * Exact traveltime (seconds) for a batch of (t0, dx_s, dy_s, dx_r, dy_r, v, eta)
- * rows -- the surrogate network's training target and judge.  kind as above;
+ * rows -- the surrogate network's training target and yardstick.  kind as above;
  * curved-ray parameters shared.  out[i] = T.
  */
 void pstm_oracle_traveltime(int32_t kind, int64_t n, const double *feat7,
