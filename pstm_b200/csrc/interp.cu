@@ -31,6 +31,12 @@ using namespace pstm::ctx;
 namespace {
 
 constexpr int kInterpThreads = 128;
+// CTAs per SM the register budget is sized for: the kernel is bound by
+// dependent FP64 latency, so more resident warps beat the few values that
+// spill to L1 at this budget.
+#ifndef PSTM_INTERP_MIN_CTAS
+#define PSTM_INTERP_MIN_CTAS 8
+#endif
 
 template <int AMP>
 __device__ inline double sample_at(const unsigned char *row, int64_t i) {
@@ -147,7 +153,7 @@ struct Staged {
 };
 
 template <int AMP, int HW, bool LANCZOS>
-__global__ void __launch_bounds__(kInterpThreads) migrate_interp_kernel(const KParams P, int tt, int method) {
+__global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_interp_kernel(const KParams P, int tt, int method) {
     __shared__ Staged S;
     const int p = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
