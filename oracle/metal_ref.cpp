@@ -12,6 +12,8 @@
 //   pstm_migration.metal       pstm_migrate_3d         (straight rays, AA, 1-D or 3-D velocity)
 //   pstm_curved_ray.metal      pstm_migrate_curved_ray (V(z) = v0 + k z)
 //   pstm_anisotropic_vti.metal pstm_migrate_vti        (eta moveout)
+//   pstm_migration.metal       pstm_migrate_time_variant (straight rays at the
+//                              sample times of time-variant windows)
 // The helpers (AA weight, DSR, curved and VTI traveltimes) are exported too.
 #include <metal_stdlib>
 
@@ -158,6 +160,44 @@ void pstm_ref_migrate_vti(const pstm_ref_call *c) {
                 ref_vti::pstm_migrate_vti(c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, fold,
                                           c->x_coords, c->y_coords, c->t0_s, c->inv_v_sq, c->apertures, c->eta, p,
                                           uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
+}
+
+// Time-variant form: windows as the shader's TimeWindow records (t_start_ms,
+// t_end_ms, dt_effective_ms as float; downsample_factor, sample_offset,
+// n_samples as int32), velocity at the base sampling c->dt_ms (nt_base values,
+// or nx * ny * nt_base with use_3d_velocity); image and fold are (nx, ny,
+// total samples of the windows).  c->t0_s, t0_half_sq, apertures, eta and
+// inv_v_sq are not used.
+void pstm_ref_migrate_time_variant(const pstm_ref_call *c, const float *vrms_base, int32_t nt_base,
+                                   const ref_straight::TimeWindow *windows, int32_t n_windows) {
+    ref_straight::TimeVariantParams p{};
+    p.dx = c->dx;
+    p.dy = c->dy;
+    p.dt_base_ms = c->dt_ms;
+    p.t_start_ms = c->t_start_ms;
+    p.max_aperture = c->max_aperture;
+    p.min_aperture = c->min_aperture;
+    p.taper_fraction = c->taper_fraction;
+    p.max_dip_deg = c->max_dip_deg;
+    p.apply_spreading = c->spreading;
+    p.apply_obliquity = c->obliquity;
+    p.apply_aa = c->aa;
+    p.aa_dominant_freq = c->aa_dominant_freq;
+    p.n_traces = c->n_traces;
+    p.n_samples = c->n_samples;
+    p.nx = c->nx;
+    p.ny = c->ny;
+    p.n_windows = n_windows;
+    p.total_output_samples = c->nt;
+    p.use_3d_velocity = c->use_3d_velocity;
+    p.nt_base = nt_base;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int ix = 0; ix < c->nx; ++ix)
+        for (int iy = 0; iy < c->ny; ++iy)
+            for (int it = 0; it < c->nt; ++it)
+                ref_straight::pstm_migrate_time_variant(c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image,
+                                                        c->fold, c->x_coords, c->y_coords, vrms_base, windows, p,
+                                                        uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
 }
 
 }  // extern "C"

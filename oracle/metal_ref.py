@@ -42,6 +42,12 @@ class Call(ctypes.Structure):
                                   "taper_fraction", "max_dip_deg", "aa_dominant_freq", "v0", "k", "eta_constant")]
 
 
+class Window(ctypes.Structure):
+    """Mirror of the shader's TimeWindow (pstm_migration.metal:495-502)."""
+    _fields_ = [("t_start_ms", _f), ("t_end_ms", _f), ("dt_effective_ms", _f), ("downsample_factor", ctypes.c_int32),
+                ("sample_offset", ctypes.c_int32), ("n_samples", ctypes.c_int32)]
+
+
 def build(reference_root: str | None = None) -> str | None:
     """Build the library from the reference tree; None when the tree is absent."""
     ref = reference_root or os.environ.get("PSTM_REFERENCE", "/root/reference")
@@ -76,6 +82,9 @@ def lib():
         for name in ("pstm_ref_migrate_straight", "pstm_ref_migrate_curved", "pstm_ref_migrate_vti"):
             getattr(L, name).argtypes = [ctypes.POINTER(Call)]
             getattr(L, name).restype = None
+        L.pstm_ref_migrate_time_variant.argtypes = [ctypes.POINTER(Call), _pf, ctypes.c_int32,
+                                                    ctypes.POINTER(Window), ctypes.c_int32]
+        L.pstm_ref_migrate_time_variant.restype = None
         _lib = L
     return _lib
 
@@ -156,4 +165,47 @@ def migrate(kind: str, amps, sx, sy, rx, ry, x_coords, y_coords, t_axis_ms, vrms
           "vti": lib().pstm_ref_migrate_vti}[kind]
     fn(ctypes.byref(c))
     del keep
+    return image, fold
+
+
+def migrate_time_variant(amps, sx, sy, rx, ry, x_coords, y_coords, vrms_base, windows, *, aperture_m: float,
+                         taper: float, dx: float, dy: float, dt_ms: float, t_start_ms: float = 0.0, spreading=True,
+                         obliquity=True, aa=True, aa_dominant_freq=30.0, max_dip_deg=45.0):
+    """Image (nx, ny, n_windowed) FP32 and per-sample fold of
+    pstm_migrate_time_variant (pstm_migration.metal:544-701).
+
+    ``windows`` are ``pstm_b200.time_variant.TimeWindow`` records;
+    ``vrms_base`` is v_rms at the trace sampling ``dt_ms`` ((nt_base) or
+    (nx, ny, nt_base)).  The shader's aperture is min(max, min + v t / 2);
+    ``aperture_m`` sets both ends, so it is that value at every time.
+    """
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    amps = f32(amps)
+    n_traces, ns = amps.shape
+    mx = f32((np.asarray(sx, np.float64) + np.asarray(rx, np.float64)) / 2.0)
+    my = f32((np.asarray(sy, np.float64) + np.asarray(ry, np.float64)) / 2.0)
+    sx, sy, rx, ry = f32(sx), f32(sy), f32(rx), f32(ry)
+    xc, yc = f32(x_coords).ravel(), f32(y_coords).ravel()
+    nx, ny = np.shape(x_coords)
+    v = f32(vrms_base)
+    use3d = v.ndim == 3
+    nt_base = v.shape[-1]
+    win = (Window * max(1, len(windows)))()
+    for i, w in enumerate(windows):
+        win[i] = Window(w.t_start_ms, w.t_end_ms, w.dt_effective_ms, w.downsample_factor, w.sample_start,
+                        w.n_samples)
+    total = int(sum(w.n_samples for w in windows))
+    image = np.zeros((nx, ny, total), np.float32)
+    fold = np.zeros((nx, ny, total), np.int32)
+    c = Call()
+    ptr = lambda a: a.ctypes.data_as(_pf)
+    c.amps, c.sx, c.sy, c.rx, c.ry, c.mx, c.my = map(ptr, (amps, sx, sy, rx, ry, mx, my))
+    c.x_coords, c.y_coords, c.image = ptr(xc), ptr(yc), ptr(image)
+    c.fold = fold.ctypes.data_as(_pi)
+    c.n_traces, c.n_samples, c.nx, c.ny, c.nt = n_traces, ns, nx, ny, total
+    c.spreading, c.obliquity, c.aa, c.use_3d_velocity = int(spreading), int(obliquity), int(aa), int(use3d)
+    c.dx, c.dy, c.dt_ms, c.t_start_ms = dx, dy, dt_ms, t_start_ms
+    c.max_aperture = c.min_aperture = aperture_m
+    c.taper_fraction, c.max_dip_deg, c.aa_dominant_freq = taper, max_dip_deg, aa_dominant_freq
+    lib().pstm_ref_migrate_time_variant(ctypes.byref(c), ptr(v), nt_base, win, len(windows))
     return image, fold

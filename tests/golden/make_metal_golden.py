@@ -10,11 +10,13 @@ container that has the reference:
 
     PSTM_REFERENCE=/path/to/reference python tests/golden/make_metal_golden.py
 
-The tests read only the .npz.  All inputs are FP32-exact (the shaders take
-FP32), so the FP64 oracle sees the same numbers.  The aperture table is one
-constant (min_aperture = max_aperture): the Metal host's per-time aperture
-law is not under test here (the straight-ray law is pinned to the
-reference's Numba kernel by make_golden.py).
+A sixth run is the time-variant shader (pstm_migrate_time_variant) at the
+windows of a seeded frequency table, 3-D velocity, AA on.  The tests read
+only the .npz.  All inputs are FP32-exact (the shaders take FP32), so the
+FP64 oracle sees the same numbers.  The aperture is one constant
+(min_aperture = max_aperture): the Metal host's per-time aperture law is not
+under test here (the straight-ray law is pinned to the reference's Numba
+kernel by make_golden.py).
 """
 from __future__ import annotations
 
@@ -69,6 +71,21 @@ def run_case(mr, d, spec):
                       eta_constant=eta if isinstance(eta, float) else 0.0)
 
 
+TV_TABLE = ([0.0, 150.0, 300.0, 476.0], [80.0, 60.0, 25.0, 12.0])   # (ms, Hz)
+
+
+def tv_windows():
+    """Time-variant windows over the case's output axis at the 4 ms base rate."""
+    from pstm_b200 import time_variant as tvm
+    table = tvm.FrequencyTimeTable(times_ms=TV_TABLE[0], frequencies_hz=TV_TABLE[1])
+    return tvm.compute_time_windows(0.0, (NT - 1) * DT_MS + DT_MS, DT_MS, table)
+
+
+def run_tv(mr, d):
+    return mr.migrate_time_variant(d["amps"], d["sx"], d["sy"], d["rx"], d["ry"], d["X"], d["Y"], d["v3"],
+                                   tv_windows(), aperture_m=APERTURE, taper=TAPER, dx=DX, dy=DX, dt_ms=DT_MS)
+
+
 def helper_rows(mr):
     """Curved-ray and VTI two-leg traveltimes at seeded (t0, h_s, h_r, v, eta)."""
     rng = np.random.default_rng(11)
@@ -93,6 +110,7 @@ def main():
     for spec in CASES:
         img, fold = run_case(mr, d, spec)
         res[f"{spec[0]}_image"], res[f"{spec[0]}_fold"] = img, fold
+    res["tv_image"], res["tv_fold"] = run_tv(mr, d)
     res.update(helper_rows(mr))
     np.savez_compressed(OUT, **res)
     print(f"wrote {OUT} ({os.path.getsize(OUT)} bytes)")

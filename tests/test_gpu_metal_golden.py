@@ -7,7 +7,8 @@ on FP32-exact inputs with a constant aperture.  The CUDA backend, through
 its public methods on host arrays, must reproduce their images within the
 tolerances of the same kinds against the FP64 oracle (1e-5 straight rays on
 the exact path, 1e-4 curved and VTI on the FP32 traveltime path), and the
-curved and VTI kernels' (nx, ny) fold exactly."""
+curved and VTI kernels' (nx, ny) fold exactly.  The time-variant shader's
+image at the window times is reproduced by ``migrate_tile_time_variant``."""
 from __future__ import annotations
 
 import os
@@ -57,3 +58,20 @@ def test_cuda_matches_metal_kernel(spec, cuda_kernel_factory):
     assert rel_l2(out.image, ref) <= TOL[kind]
     if kind != "straight":
         np.testing.assert_array_equal(out.fold, d[f"{name}_fold"])
+
+
+def test_cuda_time_variant_matches_metal_kernel(cuda_kernel_factory):
+    from pstm_b200.base import KernelConfig, OutputTile, VelocitySlice, create_trace_block
+    d = dict(np.load(FIXTURE))
+    f64 = lambda a: np.asarray(a, np.float64)
+    tb = create_trace_block(d["amps"], f64(d["sx"]), f64(d["sy"]), f64(d["rx"]), f64(d["ry"]),
+                            sample_rate_ms=G.DT_MS)
+    out = OutputTile(image=np.zeros((G.NX, G.NY, G.NT)), fold=np.zeros((G.NX, G.NY), np.int32),
+                     x_axis=f64(d["X"][:, 0]), y_axis=f64(d["Y"][0, :]), t_axis_ms=f64(d["t_ms"]))
+    cfg = KernelConfig(max_aperture_m=G.APERTURE, min_aperture_m=G.APERTURE, max_dip_degrees=45.0,
+                       taper_fraction=G.TAPER, aa_enabled=True, grid_dx=G.DX, grid_dy=G.DX, aa_dominant_freq=30.0)
+    kern = cuda_kernel_factory(cfg)
+    kern.migrate_tile_time_variant(tb, out, VelocitySlice(vrms=f64(d["v3"]), is_1d=False), cfg, G.tv_windows())
+    ref = d["tv_image"].astype(np.float64)
+    assert out.image.shape == ref.shape
+    assert rel_l2(out.image, ref) <= TOL["straight"]

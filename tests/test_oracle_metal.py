@@ -3,8 +3,9 @@
 ``tests/golden/metal_kernels.npz`` holds inputs and outputs of the
 reference's own shader kernels -- pstm_migrate_3d (straight rays, AA, 1-D and
 3-D velocity, rotated grid, start time > 0), pstm_migrate_curved_ray and
-pstm_migrate_vti (eta(t) and constant eta) -- and of their curved-ray and VTI
-traveltime helpers, compiled unchanged as C++ and run on the CPU by
+pstm_migrate_vti (eta(t) and constant eta), pstm_migrate_time_variant (at the
+windows of a frequency table) -- and of their curved-ray and VTI traveltime
+helpers, compiled unchanged as C++ and run on the CPU by
 ``tests/golden/make_metal_golden.py``.  The FP64 oracle must reproduce the
 FP32 shaders' images to FP32 accuracy (relative L2 bounds below) and, for
 the curved and VTI kernels, their (nx, ny) fold exactly.  The straight
@@ -73,6 +74,29 @@ def test_oracle_matches_metal_kernel(spec, fx):
         assert out.fold.min() > 0
 
 
+def test_oracle_matches_metal_time_variant_kernel(fx):
+    """The shader migrates at the window times with v_rms at the base sample at
+    or below each time; the windows start on base samples, so that is the
+    oracle on the windowed time axis with v_rms taken there."""
+    from pstm_b200 import time_variant as tvm
+    from pstm_b200.base import KernelConfig, OutputTile, VelocitySlice, create_trace_block
+    f64 = lambda a: np.asarray(a, np.float64)
+    tv = tvm.window_times(G.tv_windows())
+    assert len(tv) == fx["tv_image"].shape[-1] and np.allclose(tv % G.DT_MS, 0.0)
+    v3 = f64(fx["v3"])
+    vel = v3[..., np.minimum((tv / G.DT_MS).astype(int), v3.shape[-1] - 1)]
+    tb = create_trace_block(fx["amps"], f64(fx["sx"]), f64(fx["sy"]), f64(fx["rx"]), f64(fx["ry"]),
+                            sample_rate_ms=G.DT_MS)
+    out = OutputTile(image=np.zeros((G.NX, G.NY, len(tv))), fold=np.zeros((G.NX, G.NY), np.int32),
+                     x_axis=f64(fx["X"][:, 0]), y_axis=f64(fx["Y"][0, :]), t_axis_ms=tv)
+    cfg = KernelConfig(max_aperture_m=G.APERTURE, min_aperture_m=G.APERTURE, max_dip_degrees=45.0,
+                       taper_fraction=G.TAPER, aa_enabled=True, grid_dx=G.DX, grid_dy=G.DX, aa_dominant_freq=30.0)
+    oracle.migrate(tb, out, VelocitySlice(vrms=vel, is_1d=False), cfg)
+    ref = fx["tv_image"].astype(np.float64)
+    assert np.abs(ref).max() > 0
+    assert rel_l2(out.image, ref) <= TOL["straight"]
+
+
 def test_traveltime_helpers_match_metal(fx):
     """Two-leg curved-ray and VTI traveltimes: within 2 us of the FP32 shader
     helpers (1e-3 of a 2 ms sample; the shaders' FP32 log of a ratio near 1
@@ -96,6 +120,9 @@ def test_fixture_is_the_shaders_output():
         img, fold = G.run_case(metal_ref, d, spec)
         np.testing.assert_array_equal(img, d[f"{spec[0]}_image"])
         np.testing.assert_array_equal(fold, d[f"{spec[0]}_fold"])
+    img, fold = G.run_tv(metal_ref, d)
+    np.testing.assert_array_equal(img, d["tv_image"])
+    np.testing.assert_array_equal(fold, d["tv_fold"])
     h = G.helper_rows(metal_ref)
     for key, val in h.items():
         np.testing.assert_array_equal(val, d[key])
