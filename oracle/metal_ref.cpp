@@ -9,9 +9,11 @@
 // own (they define helpers of the same names), and a migration runs the
 // shader's kernel function once per (ix, iy, it) grid position, as a Metal
 // dispatch of nx x ny x nt threads would:
-//   pstm_migration.metal       pstm_migrate_3d         (straight rays, AA, 1-D or 3-D velocity)
-//   pstm_curved_ray.metal      pstm_migrate_curved_ray (V(z) = v0 + k z)
-//   pstm_anisotropic_vti.metal pstm_migrate_vti        (eta moveout)
+//   pstm_migration.metal       pstm_migrate_3d[_simd]         (straight rays, AA, 1-D or 3-D velocity)
+//   pstm_curved_ray.metal      pstm_migrate_curved_ray[_simd] (V(z) = v0 + k z)
+//   pstm_anisotropic_vti.metal pstm_migrate_vti[_simd]        (eta moveout)
+// (`simd` picks the _simd variant, the Metal backend's default, which reads
+// the geometry of four traces at a time as float4.)
 //   pstm_migration.metal       pstm_migrate_time_variant (straight rays at the
 //                              sample times of time-variant windows)
 // The helpers (AA weight, DSR, curved and VTI traveltimes) are exported too.
@@ -71,7 +73,7 @@ float pstm_ref_vti_dsr(float t0_s, float h_s, float h_r, float v, float eta) {
     return ref_vti::vti_dsr_traveltime(t0_s, h_s, h_r, v, eta);
 }
 
-void pstm_ref_migrate_straight(const pstm_ref_call *c) {
+void pstm_ref_migrate_straight(const pstm_ref_call *c, int32_t simd) {
     ref_straight::MigrationParams p{};
     p.dx = c->dx;
     p.dy = c->dy;
@@ -95,12 +97,13 @@ void pstm_ref_migrate_straight(const pstm_ref_call *c) {
     for (int ix = 0; ix < c->nx; ++ix)
         for (int iy = 0; iy < c->ny; ++iy)
             for (int it = 0; it < c->nt; ++it)
-                ref_straight::pstm_migrate_3d(c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, c->fold,
-                                              c->x_coords, c->y_coords, c->t0_half_sq, c->inv_v_sq, c->t0_s,
-                                              c->apertures, p, uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
+                (simd ? ref_straight::pstm_migrate_3d_simd : ref_straight::pstm_migrate_3d)(
+                    c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, c->fold, c->x_coords, c->y_coords,
+                    c->t0_half_sq, c->inv_v_sq, c->t0_s, c->apertures, p,
+                    uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
 }
 
-void pstm_ref_migrate_curved(const pstm_ref_call *c) {
+void pstm_ref_migrate_curved(const pstm_ref_call *c, int32_t simd) {
     ref_curved::CurvedRayParams p{};
     p.dx = c->dx;
     p.dy = c->dy;
@@ -126,12 +129,12 @@ void pstm_ref_migrate_curved(const pstm_ref_call *c) {
     for (int ix = 0; ix < c->nx; ++ix)   // fold[ix, iy] is written by the it = 0 thread only
         for (int iy = 0; iy < c->ny; ++iy)
             for (int it = 0; it < c->nt; ++it)
-                ref_curved::pstm_migrate_curved_ray(c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image,
-                                                    fold, c->x_coords, c->y_coords, c->t0_s, c->apertures, p,
-                                                    uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
+                (simd ? ref_curved::pstm_migrate_curved_ray_simd : ref_curved::pstm_migrate_curved_ray)(
+                    c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, fold, c->x_coords, c->y_coords,
+                    c->t0_s, c->apertures, p, uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
 }
 
-void pstm_ref_migrate_vti(const pstm_ref_call *c) {
+void pstm_ref_migrate_vti(const pstm_ref_call *c, int32_t simd) {
     ref_vti::VTIParams p{};
     p.dx = c->dx;
     p.dy = c->dy;
@@ -157,9 +160,9 @@ void pstm_ref_migrate_vti(const pstm_ref_call *c) {
     for (int ix = 0; ix < c->nx; ++ix)
         for (int iy = 0; iy < c->ny; ++iy)
             for (int it = 0; it < c->nt; ++it)
-                ref_vti::pstm_migrate_vti(c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, fold,
-                                          c->x_coords, c->y_coords, c->t0_s, c->inv_v_sq, c->apertures, c->eta, p,
-                                          uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
+                (simd ? ref_vti::pstm_migrate_vti_simd : ref_vti::pstm_migrate_vti)(
+                    c->amps, c->sx, c->sy, c->rx, c->ry, c->mx, c->my, c->image, fold, c->x_coords, c->y_coords,
+                    c->t0_s, c->inv_v_sq, c->apertures, c->eta, p, uint3{(unsigned)ix, (unsigned)iy, (unsigned)it});
 }
 
 // Time-variant form: windows as the shader's TimeWindow records (t_start_ms,

@@ -80,7 +80,7 @@ def lib():
                      "pstm_ref_vti_dsr"):
             getattr(L, name).restype = _f
         for name in ("pstm_ref_migrate_straight", "pstm_ref_migrate_curved", "pstm_ref_migrate_vti"):
-            getattr(L, name).argtypes = [ctypes.POINTER(Call)]
+            getattr(L, name).argtypes = [ctypes.POINTER(Call), ctypes.c_int32]
             getattr(L, name).restype = None
         L.pstm_ref_migrate_time_variant.argtypes = [ctypes.POINTER(Call), _pf, ctypes.c_int32,
                                                     ctypes.POINTER(Window), ctypes.c_int32]
@@ -118,8 +118,9 @@ def vti_dsr(t0_s, h_s, h_r, v, eta):
 def migrate(kind: str, amps, sx, sy, rx, ry, x_coords, y_coords, t_axis_ms, vrms, *, aperture_m: float,
             taper: float, dx: float, dy: float, dt_ms: float, t_start_ms: float = 0.0, spreading=True,
             obliquity=True, aa=True, aa_dominant_freq=30.0, v0=1500.0, k=0.5, eta=None, eta_constant=0.0,
-            max_dip_deg=45.0):
-    """Image (nx, ny, nt) FP32 and fold of one shader kernel.
+            max_dip_deg=45.0, simd=False):
+    """Image (nx, ny, nt) FP32 and fold of one shader kernel (``simd``: its
+    ``_simd`` variant, the Metal backend's default).
 
     ``kind`` is "straight" (pstm_migrate_3d; ``vrms`` (nt) or (nx, ny, nt)),
     "curved" (pstm_migrate_curved_ray; ``vrms`` unused) or "vti"
@@ -163,7 +164,7 @@ def migrate(kind: str, amps, sx, sy, rx, ry, x_coords, y_coords, t_axis_ms, vrms
     c.v0, c.k, c.eta_constant = v0, k, eta_constant
     fn = {"straight": lib().pstm_ref_migrate_straight, "curved": lib().pstm_ref_migrate_curved,
           "vti": lib().pstm_ref_migrate_vti}[kind]
-    fn(ctypes.byref(c))
+    fn(ctypes.byref(c), int(bool(simd)))
     del keep
     return image, fold
 

@@ -5,7 +5,8 @@ Builds ``oracle/_ref/libpstm_metal_ref.so`` -- the shaders
 ``pstm_anisotropic_vti.metal`` of the reference at REF (default
 /root/reference), compiled unchanged as C++ by ``oracle/Makefile``'s ``ref``
 target -- runs its kernels and helpers on seeded inputs and writes their
-inputs and outputs to ``tests/golden/metal_kernels.npz``.  Run it in a
+inputs and outputs to ``tests/golden/metal_kernels.npz``; every kernel runs in
+its scalar form and in its ``_simd`` form (the Metal backend's default).  Run it in a
 container that has the reference:
 
     PSTM_REFERENCE=/path/to/reference python tests/golden/make_metal_golden.py
@@ -61,14 +62,14 @@ def inputs():
         Yr=f32(700 + (X - 700) * np.sin(ang) + (Y - 700) * np.cos(ang)))
 
 
-def run_case(mr, d, spec):
+def run_case(mr, d, spec, simd=False):
     name, kind, vel, grid, t0ms, aa, spr, obl, (v0, k), eta = spec
     X, Y = (d["X"], d["Y"]) if grid == "axes" else (d["Xr"], d["Yr"])
     return mr.migrate(kind, d["amps"], d["sx"], d["sy"], d["rx"], d["ry"], X, Y, d["t_ms"],
                       d["v3"] if vel == "3d" else d["v1"], aperture_m=APERTURE, taper=TAPER, dx=DX, dy=DX,
                       dt_ms=DT_MS, t_start_ms=t0ms, spreading=bool(spr), obliquity=bool(obl), aa=bool(aa),
                       v0=v0, k=k, eta=d["eta1"] if eta == "1d" else None,
-                      eta_constant=eta if isinstance(eta, float) else 0.0)
+                      eta_constant=eta if isinstance(eta, float) else 0.0, simd=simd)
 
 
 TV_TABLE = ([0.0, 150.0, 300.0, 476.0], [80.0, 60.0, 25.0, 12.0])   # (ms, Hz)
@@ -110,6 +111,7 @@ def main():
     for spec in CASES:
         img, fold = run_case(mr, d, spec)
         res[f"{spec[0]}_image"], res[f"{spec[0]}_fold"] = img, fold
+        res[f"{spec[0]}_simd_image"], res[f"{spec[0]}_simd_fold"] = run_case(mr, d, spec, simd=True)
     res["tv_image"], res["tv_fold"] = run_tv(mr, d)
     res.update(helper_rows(mr))
     np.savez_compressed(OUT, **res)

@@ -62,15 +62,16 @@ def _oracle_case(d, spec):
     return out
 
 
+@pytest.mark.parametrize("variant", ["", "_simd"])
 @pytest.mark.parametrize("spec", G.CASES, ids=[c[0] for c in G.CASES])
-def test_oracle_matches_metal_kernel(spec, fx):
+def test_oracle_matches_metal_kernel(spec, variant, fx):
     name, kind = spec[0], spec[1]
     out = _oracle_case(fx, spec)
-    ref = fx[f"{name}_image"].astype(np.float64)
+    ref = fx[f"{name}{variant}_image"].astype(np.float64)
     assert np.abs(ref).max() > 0
     assert rel_l2(out.image, ref) <= TOL[kind]
     if kind != "straight":
-        np.testing.assert_array_equal(out.fold, fx[f"{name}_fold"])
+        np.testing.assert_array_equal(out.fold, fx[f"{name}{variant}_fold"])
         assert out.fold.min() > 0
 
 
@@ -117,9 +118,10 @@ def test_fixture_is_the_shaders_output():
         pytest.skip("the shader library is built only where the reference tree is")
     d = dict(np.load(FIXTURE))
     for spec in G.CASES:
-        img, fold = G.run_case(metal_ref, d, spec)
-        np.testing.assert_array_equal(img, d[f"{spec[0]}_image"])
-        np.testing.assert_array_equal(fold, d[f"{spec[0]}_fold"])
+        for simd, variant in ((False, ""), (True, "_simd")):
+            img, fold = G.run_case(metal_ref, d, spec, simd=simd)
+            np.testing.assert_array_equal(img, d[f"{spec[0]}{variant}_image"])
+            np.testing.assert_array_equal(fold, d[f"{spec[0]}{variant}_fold"])
     img, fold = G.run_tv(metal_ref, d)
     np.testing.assert_array_equal(img, d["tv_image"])
     np.testing.assert_array_equal(fold, d["tv_fold"])
