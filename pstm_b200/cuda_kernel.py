@@ -45,6 +45,19 @@ def _is_torch_cuda(x) -> bool:
     return hasattr(x, "is_cuda") and hasattr(x, "data_ptr") and bool(x.is_cuda)
 
 
+def lateral_velocity_choice(v3):
+    """The Metal host's choice between a 3-D velocity cube and its centre
+    pillar (``metal_compiled.py:631-664``): with max |v - v_centre| /
+    mean(v_centre) > 5 % the cube is used, else the centre pillar
+    v[nx // 2, ny // 2, :] stands for every pillar.  ``v3`` is (nx, ny, nt),
+    NumPy or torch; returns (velocity, is_3d)."""
+    nx, ny = v3.shape[0], v3.shape[1]
+    centre = v3[nx // 2, ny // 2, :]
+    rel = float((v3 - centre[None, None, :]).abs().max() / centre.mean()) if hasattr(v3, "abs") \
+        else float(np.abs(v3 - centre[None, None, :]).max() / centre.mean())
+    return (v3, True) if rel > 0.05 else (centre.contiguous() if hasattr(centre, "contiguous") else centre, False)
+
+
 def float32_to_bf16_bits(a: np.ndarray) -> np.ndarray:
     """Round-to-nearest-even FP32 -> BF16, returned as uint16 bit patterns."""
     u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
@@ -352,6 +365,9 @@ class CudaKernel:
         if _is_torch_cuda(v):
             if (is_1d and tuple(v.shape) != (nt,)) or (not is_1d and tuple(v.shape) != (nx, ny, nt)):
                 raise ValueError("device velocity must match the output tile shape")
+            if not is_1d and self._velocity_mode == "auto":
+                v, use3d = lateral_velocity_choice(v)
+                is_1d = not use3d
             return self._arr(v, np.float64, keep)[0], (0 if is_1d else 1), True
         v = np.asarray(v, dtype=np.float64)
         t_out = np.asarray(output.t_axis_ms, dtype=np.float64)
@@ -366,10 +382,8 @@ class CudaKernel:
                 raise ValueError(f"3-D velocity shape {v.shape} != tile {(nx, ny, nt)}")
             is3d = 1
             if self._velocity_mode == "auto":
-                centre = v[nx // 2, ny // 2, :]
-                rel = np.abs(v - centre[None, None, :]).max() / centre.mean()
-                if rel <= 0.05:
-                    v, is3d = centre, 0
+                v, use3d = lateral_velocity_choice(v)
+                is3d = int(use3d)
         if not np.all(v > 0):
             raise ValueError("velocity must be > 0")
         v = np.ascontiguousarray(v)
