@@ -6,7 +6,7 @@ numba_cpu.py:220-364, 584-664) from the reference checkout on one seeded
 case-1 subset (250 traces cut to 300 samples, 3 x 3 pillars, 300 output
 times) -- trace weights, time-varying aperture, taper, spreading and
 obliquity, 2-D fold -- once per non-linear method, and stores inputs and
-outputs in ``tests/golden/numba_interp_kernel.npz``.  Run once in a container
+outputs in ``tests/golden/interp_numba_kernel.npz``.  Run once in a container
 that has the reference at REF (default /root/reference):
 
     NUMBA_CACHE_DIR=/tmp/numba PYTHONDONTWRITEBYTECODE=1 \\
@@ -22,7 +22,7 @@ import numpy as np
 REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-OUT = os.path.join(HERE, "numba_interp_kernel.npz")
+OUT = os.path.join(HERE, "interp_numba_kernel.npz")
 METHODS = ["nearest", "cubic", "sinc4", "sinc8", "sinc16", "lanczos3", "lanczos5"]
 CFG = dict(max_aperture_m=1000.0, min_aperture_m=500.0, max_dip_degrees=60.0, taper_fraction=0.15,
            apply_spreading=True, apply_obliquity=True, aa_enabled=False)

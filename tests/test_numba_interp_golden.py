@@ -1,7 +1,7 @@
 """Whole migrations with the non-linear trace interpolators against the
 reference's own NumbaKernel (numba_cpu.py:220-364), whose images for nearest,
 cubic, windowed sinc 4/8/16 and Lanczos 3/5 are committed in
-``tests/golden/numba_interp_kernel.npz`` by ``make_numba_interp_golden.py``
+``tests/golden/interp_numba_kernel.npz`` by ``make_numba_interp_golden.py``
 (trace weights, time-varying aperture, taper, spreading, obliquity, 2-D fold).
 The FP64 oracle must reproduce them to 1e-10 (the reference compiles with
 fastmath), the CUDA interpolation kernel to 1e-9, the folds exactly."""
@@ -15,7 +15,7 @@ import pytest
 from conftest import rel_l2
 from oracle import oracle
 
-FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "numba_interp_kernel.npz")
+FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "interp_numba_kernel.npz")
 METHODS = ["nearest", "cubic", "sinc4", "sinc8", "sinc16", "lanczos3", "lanczos5"]
 
 
