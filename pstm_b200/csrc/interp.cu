@@ -9,11 +9,13 @@
 // the tiled gather kernel; the other methods run here, in FP64 (traveltime,
 // sample index, interpolation weights and accumulation), with one CTA of 128
 // threads per (pillar, block of 128 output times) and the traces read from
-// the packed geometry and the caller's panel.  The CTA stages the traces 128
-// at a time: each thread takes one trace's pillar distances, counts it for the
-// fold and keeps it if it lies inside the largest aperture of the CTA's times;
-// the kept traces, in trace order, go to shared memory and every thread then
-// runs them against its own output time.  Aperture, taper, weights, AA and
+// the packed geometry and the caller's panel.  Each warp stages the traces 32
+// at a time in a shared-memory slice of its own: each lane takes one trace's
+// pillar distances, counts it for the fold and keeps it if it lies inside the
+// largest aperture of the warp's times; the kept traces, in trace order, go to
+// the slice and every lane then runs them against its own output time.  Warps
+// synchronise only with themselves, so none waits for a warp whose times
+// keep more traces.  Aperture, taper, weights, AA and
 // fold are those of the gather kernel.
 #include <cuda_runtime.h>
 
@@ -143,18 +145,15 @@ __device__ inline double tt_of(double t0, double ds2, double dr2, double v, doub
     return traveltime_fp64<TT>(t0, ds2, dr2, v, eta, v0, k);
 }
 
-// Per-trace values staged in shared memory for the CTA's pillar.
+// Per-trace values a warp stages in shared memory for the CTA's pillar.
 struct Staged {
-    double ds2[kInterpThreads], dr2[kInterpThreads], d[kInterpThreads], w[kInterpThreads], m[kInterpThreads];
-    int tr[kInterpThreads];
-    int kept[kInterpThreads / 32];
-    int fold[kInterpThreads / 32];
-    double ap[kInterpThreads / 32];
+    double ds2[32], dr2[32], d[32], w[32], m[32];
+    int tr[32];
 };
 
 template <int AMP, int HW, bool LANCZOS>
 __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_interp_kernel(const KParams P, int tt, int method) {
-    __shared__ Staged S;
+    __shared__ Staged S_all[kInterpThreads / 32];
     const int p = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ix = p / P.ny, iy = p - ix * P.ny;
@@ -179,18 +178,17 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
     double sin_d = 0.0, cos_d = 1.0;
     if (HW > 0) sincospi(1.0 / (double)HW, &sin_d, &cos_d);
 
-    // Largest aperture over the CTA's output times: a trace farther than it
+    Staged &S = S_all[warp];
+    // Largest aperture over the warp's output times: a trace farther than it
     // from the pillar adds nothing at any of them.
-    double ap_cta = tv ? ap : 0.0;
+    double ap_w = tv ? ap : 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) ap_cta = fmax(ap_cta, __shfl_xor_sync(0xffffffffu, ap_cta, o));
-    if (lane == 0) { S.ap[warp] = ap_cta; S.fold[warp] = 0; }
-    __syncthreads();
-    ap_cta = fmax(fmax(S.ap[0], S.ap[1]), fmax(S.ap[2], S.ap[3]));
+    for (int o = 16; o > 0; o >>= 1) ap_w = fmax(ap_w, __shfl_xor_sync(0xffffffffu, ap_w, o));
 
     double acc = 0.0;
-    for (int64_t c0 = 0; c0 < P.n_traces; c0 += kInterpThreads) {
-        const int64_t tr = c0 + threadIdx.x;
+    int cnt = 0;   // traces within the fold radius; the same in every lane
+    for (int64_t c0 = 0; c0 < P.n_traces; c0 += 32) {
+        const int64_t tr = c0 + lane;
         bool keep = false, in_fold = false;
         double dxm = 0.0, dym = 0.0, d = 0.0;
         const double *g = P.geo + tr * kGeoDoubles;
@@ -200,19 +198,13 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             const double d2 = dxm * dxm + dym * dym;
             in_fold = d2 <= P.fold_d2_max;
             d = sqrt(d2);
-            keep = !(d > ap_cta);
+            keep = !(d > ap_w);
         }
-        const unsigned kb = __ballot_sync(0xffffffffu, keep), fb = __ballot_sync(0xffffffffu, in_fold);
-        if (lane == 0) { S.kept[warp] = __popc(kb); S.fold[warp] += __popc(fb); }
-        __syncthreads();
-        int base = 0, n_kept = 0;
-#pragma unroll
-        for (int w = 0; w < kInterpThreads / 32; ++w) {
-            base += w < warp ? S.kept[w] : 0;
-            n_kept += S.kept[w];
-        }
+        const unsigned kb = __ballot_sync(0xffffffffu, keep);
+        cnt += __popc(__ballot_sync(0xffffffffu, in_fold));
+        const int n_kept = __popc(kb);
         if (keep) {
-            const int j = base + __popc(kb & ((1u << lane) - 1u));
+            const int j = __popc(kb & ((1u << lane) - 1u));
             const double dxs = ox - g[0], dys = oy - g[1], dxr = ox - g[2], dyr = oy - g[3];
             S.ds2[j] = dxs * dxs + dys * dys;
             S.dr2[j] = dxr * dxr + dyr * dyr;
@@ -221,7 +213,7 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             S.m[j] = fmax(fabs(dxm), fabs(dym));
             S.tr[j] = (int)tr;
         }
-        __syncthreads();
+        __syncwarp();
         for (int j = 0; j < n_kept; ++j) {
             const double dj = S.d[j];
             if (!tv || dj > ap) continue;
@@ -255,9 +247,8 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             if (P.obliquity && T > 0.001) w *= t0 * inv_T;
             acc += amp * w;
         }
-        __syncthreads();   // the next batch overwrites the staged values
+        __syncwarp();   // the next batch overwrites the staged values
     }
-    const int cnt = S.fold[0] + S.fold[1] + S.fold[2] + S.fold[3];
     if (tv) {
         const int64_t idx = (int64_t)p * P.nt + t;
         if (P.image_f32) reinterpret_cast<float *>(P.image)[idx] += (float)acc;
