@@ -611,6 +611,8 @@ def main_ours(args):
     except Exception:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else \
+        "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
     roofline = {
         "bound": "sfu", "unit": "Gop/s", "achieved": achieved_mufu / 1e9, "peak": mufu_peak / 1e9,
         "frac": achieved_mufu / mufu_peak,
@@ -619,7 +621,8 @@ def main_ours(args):
         "fp32": {"achieved_tflops": pairs_per_step * FLOP_PER_PAIR / per_launch_s / 1e12,
                  "peak_tflops": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12},
         "hbm": {"achieved_gbs": alg_bytes / per_launch_s / 1e9, "peak_gbs": hbm_peak,
-                "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes},
+                "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes,
+                "peak_source": hbm_src},
         "traffic": (DRAM_BYTES_PER_TRACE_TILE64 * N / 1e9) if T == 64 else None,
         "traffic_unit": "GB per launch (ncu dram__bytes read+write of the full-size launch, scaled by traces)",
     }
