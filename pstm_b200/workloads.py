@@ -176,6 +176,31 @@ def survey(n_traces: int, nx: int, ny: int, nt: int, dt_ms: float, ns: int, dx: 
                   y_axis=np.arange(ny) * dx, t_axis_ms=t_axis, G=G, dx=dx)
 
 
+def estimate_gradient_from_vrms(vrms, t_ms, window_ms: float = 500.0) -> tuple[float, float]:
+    """(v0, k) of a linear V(z) = v0 + k z from a v_rms(t) function, as the
+    reference suggests them (``pstm/algorithm/curved_ray.py:145-201``):
+    a least-squares line v_rms ~ v0 + slope t over t <= window_ms (the first
+    len // 2 samples when fewer than two fall inside; v_rms[0] and k = 0 when
+    fewer than two remain), k = 2 slope / v0,
+    then v0 clamped to [1000, 6000] m/s and k to [0, 2] 1/s."""
+    v = np.asarray(vrms, np.float64)
+    t = np.asarray(t_ms, np.float64)
+    if len(v) < 2:
+        return (float(v[0]) if len(v) else 1500.0), 0.0
+    mask = t <= window_ms
+    if mask.sum() < 2:
+        mask = np.zeros(len(t), bool)
+        mask[:len(t) // 2] = True
+    if mask.sum() < 2:
+        return float(v[0]), 0.0
+    ts, vs = t[mask] / 1000.0, v[mask]
+    tm, vm = ts.mean(), vs.mean()
+    slope = float(((ts - tm) * (vs - vm)).sum() / ((ts - tm) ** 2).sum())
+    v0 = float(vm - slope * tm)
+    k = 2.0 * slope / v0 if v0 > 0 else 0.0
+    return max(1000.0, min(v0, 6000.0)), max(0.0, min(k, 2.0))
+
+
 def survey_config(kernel_type: str = "straight_ray", aa: bool = True, dx: float = 12.5,
                   eta: np.ndarray | None = None, v0: float = 1500.0, k: float = 0.5) -> KernelConfig:
     """Reference defaults (5 km aperture, 45 deg dip) with AA on, as cases 2-5."""
