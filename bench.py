@@ -73,6 +73,8 @@ def parse():
                     help="run the large-survey case (512x512x2000, FP16 traces, curved+VTI) instead")
     ap.add_argument("--case5-tiles", type=int, default=2, help="64x64 tiles of the case-5 grid to migrate")
     ap.add_argument("--case5-aperture", type=float, default=1000.0, help="max aperture (m) of the case-5 run")
+    ap.add_argument("--no-numba", action="store_true", help="skip the reference's Numba CPU leg")
+    ap.add_argument("--numba-leg", default=None, help=argparse.SUPPRESS)   # internal: the child process
     ap.add_argument("--batch-scale", type=int, default=16,
                     help="the batched form migrates 1/this of every bin's traces (1: the full ~2M traces)")
     return ap.parse_args()
@@ -90,6 +92,195 @@ def tiles_of(tile):
 def config():
     from pstm_b200 import workloads
     return workloads.survey_config(kernel_type="straight_ray", aa=True, dx=DX)
+
+
+def measured_sfu_peak(device: int) -> float:
+    """MUFU operations/s of this GPU from the library's throughput kernel (0 on failure)."""
+    import ctypes
+    from pstm_b200 import _native as nat
+    L = nat.load()
+    v = ctypes.c_double(0.0)
+    if L.pstm_cuda_measure_sfu_peak(device, ctypes.byref(v)) != nat.OK:
+        return 0.0
+    return float(v.value)
+
+
+# ------------------------------------------------------------------ the reference's Numba path
+REF_PKG = os.path.join(ROOT, "baseline", "_ref")
+C2_SAMPLE = dict(n_traces=1 << 16, pillars=16)   # labelled case-2 sample of the Numba leg
+
+
+def c2_numba_sample():
+    """The case-2 sample the reference's Numba kernel can run: the first 65,536
+    traces of the seeded case-2 survey (1500 samples at 2 ms), the 16 x 16
+    pillars at the centre of the grid x 1500 output samples, the centre
+    pillar's v_rms as a 1-D velocity (Numba takes no 3-D velocity), AA off
+    (Numba has none), reference defaults otherwise (5 km aperture, 45 deg dip).
+    Returns (traces, x_axis, y_axis, t_axis, vrms, config) as plain arrays."""
+    from pstm_b200 import workloads
+    n, pb = C2_SAMPLE["n_traces"], C2_SAMPLE["pillars"]
+    sv = workloads.survey(n, GRID, GRID, NT, DT_MS, NS, dx=DX, seed=7)
+    c0 = GRID // 2 - pb // 2
+    xa, ya = sv.x_axis[c0:c0 + pb].copy(), sv.y_axis[c0:c0 + pb].copy()
+    v = np.ascontiguousarray(sv.velocity(GRID // 2, GRID // 2 + 1, GRID // 2, GRID // 2 + 1)[0, 0])
+    cfg = workloads.survey_config(kernel_type="straight_ray", aa=False, dx=DX)
+    return sv, xa, ya, sv.t_axis_ms.copy(), v, cfg
+
+
+def _to_reference(rb, amps, sx, sy, rx, ry, dt_ms, xa, ya, ta, vrms, cfg):
+    import dataclasses
+    tb = rb.create_trace_block(np.ascontiguousarray(amps, np.float32), sx, sy, rx, ry, sample_rate_ms=dt_ms,
+                               start_time_ms=0.0)
+    out = rb.OutputTile(image=np.zeros((len(xa), len(ya), len(ta))), fold=np.zeros((len(xa), len(ya), len(ta)),
+                                                                                      np.int32),
+                        x_axis=xa, y_axis=ya, t_axis_ms=ta)
+    vel = rb.VelocitySlice(vrms=np.ascontiguousarray(vrms, np.float64), is_1d=True)
+    names = {f.name for f in dataclasses.fields(rb.KernelConfig)}
+    kw = {f.name: getattr(cfg, f.name) for f in dataclasses.fields(cfg) if f.name in names}
+    return tb, out, vel, rb.KernelConfig(**kw)
+
+
+def numba_leg_child(outdir):
+    """Child process of :func:`numba_reference`: times the reference's own
+    registered CPU backend, OptimizedNumbaKernel.migrate_tile
+    (pstm/kernels/numba_cpu_optimized.py:545-626), from the installed reference
+    in baseline/_ref, on every host core, after a JIT warm-up call with the
+    same array ranks; saves its images for the parity check."""
+    sys.path.insert(0, REF_PKG)
+    import numba
+    from pstm.kernels import base as rb
+    from pstm.kernels.numba_cpu_optimized import OptimizedNumbaKernel
+    from pstm_b200 import workloads
+    numba.set_num_threads(os.cpu_count())
+    res = {"threads": numba.get_num_threads(), "cores": os.cpu_count(), "numba": numba.__version__,
+           "cpu_model": _cpu_model()}
+    case = workloads.config1()
+    tbc = case.traces
+    args1 = (tbc.amplitudes, tbc.source_x, tbc.source_y, tbc.receiver_x, tbc.receiver_y, tbc.sample_rate_ms,
+             case.output.x_axis, case.output.y_axis, case.output.t_axis_ms, case.velocity.vrms, case.config)
+    k = OptimizedNumbaKernel()
+    # warm-up: the same array ranks (3-D fold) on 2 x 2 pillars and 64 traces
+    w = _to_reference(rb, tbc.amplitudes[:64], tbc.source_x[:64], tbc.source_y[:64], tbc.receiver_x[:64],
+                      tbc.receiver_y[:64], tbc.sample_rate_ms, case.output.x_axis[:2], case.output.y_axis[:2],
+                      case.output.t_axis_ms, case.velocity.vrms, case.config)
+    t0 = time.perf_counter()
+    k.initialize(w[3])
+    k.migrate_tile(*w)
+    res["jit_warmup_s"] = time.perf_counter() - t0
+    tb, out, vel, cfg = _to_reference(rb, *args1)
+    k.initialize(cfg)
+    t0 = time.perf_counter()
+    k.migrate_tile(tb, out, vel, cfg)
+    dt = time.perf_counter() - t0
+    res["case1"] = {"value": case.pairs / dt, "unit": UNIT, "seconds": dt, "pairs": case.pairs,
+                    "workload": "case 1 in full: 64x64x500 @4 ms, 16,384 FP32 traces x 500, straight rays, "
+                                "1000 m aperture, 60 deg dip, weights on, AA off"}
+    np.savez(os.path.join(outdir, "numba_case1.npz"), image=out.image, fold=out.fold)
+    sv, xa, ya, ta, v, c2cfg = c2_numba_sample()
+    tb, out, vel, cfg = _to_reference(rb, sv.amps, sv.s[:, 0], sv.s[:, 1], sv.r[:, 0], sv.r[:, 1], DT_MS, xa, ya,
+                                      ta, v, c2cfg)
+    k.initialize(cfg)
+    t0 = time.perf_counter()
+    k.migrate_tile(tb, out, vel, cfg)
+    dt = time.perf_counter() - t0
+    pairs = len(xa) * len(ya) * len(ta) * sv.amps.shape[0]
+    res["case2_sample"] = {"value": pairs / dt, "unit": UNIT, "seconds": dt, "pairs": pairs,
+                           "workload": f"case-2 sample: {len(xa)}x{len(ya)} centre pillars x {len(ta)} @2 ms, "
+                                       f"{sv.amps.shape[0]} traces x {NS}; centre-pillar 1-D v_rms, AA off "
+                                       "(Numba supports neither 3-D velocity nor AA), 5 km aperture"}
+    np.savez(os.path.join(outdir, "numba_case2_sample.npz"), image=out.image, fold=out.fold)
+    k.cleanup()
+    print("NUMBA_LEG " + json.dumps(res), flush=True)
+
+
+def numba_comparison(outdir):
+    """The reference's Numba path beside the CUDA kernel on the same inputs:
+    its timings (child process, all host cores) and, on the GPU, the CUDA
+    backend on the identical case-1 tile and case-2 sample -- rate (CUDA
+    events, device-resident inputs), fold equality and image relative L2
+    against the Numba images."""
+    import torch
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, TraceBlock, VelocitySlice
+    from pstm_b200.cuda_kernel import CudaKernel
+    res = numba_reference(outdir)
+    if "unavailable" in res:
+        return res
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+
+    def cuda_run(amps, sx, sy, rx, ry, dt_ms, xa, ya, ta, vrms, cfg, reps):
+        mx, my = (sx + rx) / 2.0, (sy + ry) / 2.0
+        tb = TraceBlock(amplitudes=dev(np.asarray(amps, np.float32)), source_x=dev(sx), source_y=dev(sy),
+                        receiver_x=dev(rx), receiver_y=dev(ry), offset=dev(np.hypot(rx - sx, ry - sy)),
+                        midpoint_x=dev(mx), midpoint_y=dev(my), sample_rate_ms=dt_ms, start_time_ms=0.0)
+        shape = (len(xa), len(ya), len(ta))
+        mk = lambda: OutputTile(image=torch.zeros(shape, dtype=torch.float64, device="cuda"),
+                                fold=torch.zeros(shape, dtype=torch.int32, device="cuda"), x_axis=dev(xa),
+                                y_axis=dev(ya), t_axis_ms=dev(ta))
+        vel = VelocitySlice(vrms=dev(vrms), is_1d=True)
+        k = CudaKernel()
+        k.initialize(cfg)
+        o = mk()
+        k.migrate_tile(tb, o, vel)   # the compared result (one call)
+        k.synchronize()
+        img, fold = o.image.cpu().numpy(), o.fold.cpu().numpy()
+        scratch = mk()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            k.migrate_tile(tb, scratch, vel)
+        e1.record()
+        torch.cuda.synchronize()
+        k.cleanup()
+        return img, fold, e0.elapsed_time(e1) / reps
+
+    def compare(name, img, fold):
+        z = np.load(os.path.join(outdir, name))
+        ref = z["image"]
+        return {"fold_equal": bool(np.array_equal(fold, z["fold"])),
+                "image_rel_l2": float(np.linalg.norm(img - ref) / np.linalg.norm(ref))}
+
+    case = workloads.config1()
+    tb = case.traces
+    img, fold, ms = cuda_run(tb.amplitudes, tb.source_x, tb.source_y, tb.receiver_x, tb.receiver_y,
+                             tb.sample_rate_ms, case.output.x_axis, case.output.y_axis, case.output.t_axis_ms,
+                             case.velocity.vrms, case.config, 10)
+    res["case1"]["cuda"] = {"value": case.pairs / (ms / 1e3), "ms": ms, **compare("numba_case1.npz", img, fold)}
+    res["case1"]["cuda_over_numba"] = res["case1"]["cuda"]["value"] / res["case1"]["value"]
+    sv, xa, ya, ta, v, cfg = c2_numba_sample()
+    img, fold, ms = cuda_run(sv.amps, sv.s[:, 0], sv.s[:, 1], sv.r[:, 0], sv.r[:, 1], DT_MS, xa, ya, ta, v, cfg, 5)
+    c2 = res["case2_sample"]
+    c2["cuda"] = {"value": c2["pairs"] / (ms / 1e3), "ms": ms, **compare("numba_case2_sample.npz", img, fold)}
+    c2["cuda_over_numba"] = c2["cuda"]["value"] / c2["value"]
+    return res
+
+
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def numba_reference(outdir, timeout_s=900):
+    """Run :func:`numba_leg_child` in a fresh process (Numba's thread pool and
+    torch's stay apart); None when the reference is not installed."""
+    if not os.path.isdir(os.path.join(REF_PKG, "pstm")):
+        return {"unavailable": "the reference is not installed in baseline/_ref"}
+    env = dict(os.environ, NUMBA_NUM_THREADS=str(os.cpu_count()), PYTHONDONTWRITEBYTECODE="1",
+               NUMBA_CACHE_DIR=os.path.join(outdir, "numba_cache"))
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--numba-leg", outdir], env=env,
+                           capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"the Numba leg exceeded {timeout_s} s"}
+    for line in r.stdout.splitlines():
+        if line.startswith("NUMBA_LEG "):
+            return json.loads(line[len("NUMBA_LEG "):])
+    return {"unavailable": f"the Numba leg failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"}
 
 
 # ------------------------------------------------------------------ clocks
@@ -602,7 +793,11 @@ def main_ours(args):
     # geometry-packing kernels of a step take ~1e-4 of it)
     per_launch_s = ms / 1e3 / args.steps
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    mufu_peak = 148 * 16 * sm_mhz * 1e6          # MUFU ops/s, derived: 148 SMs x 16/clk x median SM clock
+    mufu_derived = 148 * 16 * sm_mhz * 1e6       # MUFU ops/s: 148 SMs x 16/clk x median SM clock
+    mufu_peak, mufu_src = measured_sfu_peak(local), "measured: MUFU-throughput kernel on this GPU " \
+        "(sqrt.approx/rcp.approx chains, full occupancy, CUDA events, best of 3), same run"
+    if not mufu_peak:
+        mufu_peak, mufu_src = mufu_derived, "derived: 148 SMs x 16 MUFU/clk x median SM clock under load"
     achieved_mufu = pairs_per_step * MUFU_PER_PAIR / per_launch_s
     elem = amps.element_size()
     alg_bytes = N * NS * elem + N * 6 * 8 + T * T * NT * (8 + 8 + 4 + 4) + T * T * NT * 8
@@ -617,7 +812,7 @@ def main_ours(args):
     roofline = {
         "bound": "sfu", "unit": "Gop/s", "achieved": achieved_mufu / 1e9, "peak": mufu_peak / 1e9,
         "frac": achieved_mufu / mufu_peak,
-        "peak_source": "derived: 148 SMs x 16 MUFU/clk x median SM clock under load (no measured SFU peak)",
+        "peak_source": mufu_src, "peak_derived": mufu_derived / 1e9,
         "per_pair": f"{FLOP_PER_PAIR} FP32 FLOP + {MUFU_PER_PAIR} MUFU (straight-ray DSR + AA + weights)",
         "fp32": {"achieved_tflops": pairs_per_step * FLOP_PER_PAIR / per_launch_s / 1e12,
                  "peak_tflops": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12},
@@ -681,6 +876,12 @@ def main_ours(args):
         forms = forms or {}
         forms["learned_vti"] = measure_learned(args, sv, amps, world, dist)
 
+    numba_line = None
+    if single and not args.no_numba:
+        import tempfile
+        with tempfile.TemporaryDirectory(prefix="pstm_numba_") as td:
+            numba_line = numba_comparison(td)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
@@ -707,6 +908,7 @@ def main_ours(args):
                        "l2": "inputs larger than L2 (trace panel > 126 MB), no flush",
                        "parallelism": f"replicas x{world} (disjoint tiles)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "forms": forms,
+            "reference_numba": numba_line,
             "gpu_launches": 3 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -841,6 +1043,9 @@ def main_case5(args):
 
 def main():
     args = parse()
+    if args.numba_leg:
+        numba_leg_child(args.numba_leg)
+        return
     if args.case5:
         main_case5(args)
         return

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define PSTM_CUDA_ABI_VERSION 4
+#define PSTM_CUDA_ABI_VERSION 5
 
 typedef enum {
     PSTM_OK = 0,
@@ -191,11 +191,22 @@ int32_t pstm_cuda_migrate_tile_host(void *ctx, const pstm_traces_desc *traces,
  * on `stream` (NULL = the legacy default stream) of the calling thread's
  * current device.  The first call on a device looks up the array's address;
  * make that first call before any stream capture.  All calls share the array,
- * so calls that overlap on the GPU race: serialise them.  Errors are reported
- * by pstm_cuda_last_error(NULL). */
+ * so calls that overlap on the GPU race: serialise them.  The call is
+ * asynchronous: its return status covers argument checks and launches, and
+ * device-side failures are read afterwards with pstm_cuda_noalloc_status.
+ * Messages are reported by pstm_cuda_last_error(NULL). */
 int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *traces, const pstm_output_desc *output,
                                        const pstm_velocity_desc *velocity, const pstm_params *params,
                                        void *stream);
+
+/* Device-side status of the last pstm_cuda_migrate_tile_noalloc call on the
+ * current device (no reference counterpart; the allocation-free form has
+ * none).  Waits for `stream` (NULL = the legacy default stream), then reads the
+ * kernel's error word from the fixed scratch array without allocating:
+ * PSTM_OK, or PSTM_ERR_TIMEOUT when a bounded device-side wait gave up -- the
+ * image and fold of that call may then hold partial sums and must be
+ * discarded.  Each allocation-free call clears the word when it starts. */
+int32_t pstm_cuda_noalloc_status(void *stream);
 
 /* One output of the batched form: a contiguous range of the batch's traces and
  * its own image and fold.  Reference: one bin of the gather-bin loop,
@@ -323,6 +334,14 @@ int32_t pstm_cuda_migrate_tile_learned_dev(void *ctx, const pstm_traces_desc *tr
 int32_t pstm_cuda_interp_rows(void *ctx, int32_t dtype, const void *src, int64_t n_rows, int32_t n_src,
                               const double *src_times, int32_t n_dst, const double *dst_times, void *dst,
                               void *stream);
+
+/* Measured MUFU (special-function unit) throughput of `device`, in operations
+ * per second: a full-occupancy grid of independent sqrt.approx / rcp.approx
+ * chains, timed with CUDA events (best of three after a warm-up).  No
+ * reference counterpart: the denominator of the gather kernel's roofline, whose
+ * per-pair work is counted in MUFU operations.  Synchronous; allocates a
+ * small sink buffer. */
+int32_t pstm_cuda_measure_sfu_peak(int32_t device, double *ops_per_second);
 
 /* Wait for all work queued on the context's stream.  Replaces
  * MigrationKernel.synchronize, pstm/kernels/base.py:315. */

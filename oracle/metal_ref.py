@@ -48,9 +48,10 @@ class Window(ctypes.Structure):
                 ("sample_offset", ctypes.c_int32), ("n_samples", ctypes.c_int32)]
 
 
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def build(reference_root: str | None = None) -> str | None:
     """Build the library from the reference tree; None when the tree is absent."""
-    ref = reference_root or os.environ.get("PSTM_REFERENCE", "/root/reference")
+    ref = reference_root or os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
     if not os.path.isdir(os.path.join(ref, "pstm", "metal", "shaders")):
         return None
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)

@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpstm_cuda.so")
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # pstm_status
 OK, ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_NOT_INITIALIZED, \
@@ -133,6 +133,7 @@ SIGNATURES = {
                                                      ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
     "pstm_cuda_migrate_tile_noalloc": (ctypes.c_int32, [ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                         ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
+    "pstm_cuda_noalloc_status": (ctypes.c_int32, [_vp]),
     "pstm_cuda_migrate_bins_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                     ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params),
                                                     ctypes.POINTER(BinDesc), ctypes.c_int32, _vp]),
@@ -154,6 +155,7 @@ SIGNATURES = {
                                                             ctypes.POINTER(LearnedReport), _vp]),
     "pstm_cuda_interp_rows": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, ctypes.c_int32, _vp,
                                                ctypes.c_int32, _vp, _vp, _vp]),
+    "pstm_cuda_measure_sfu_peak": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),
 }

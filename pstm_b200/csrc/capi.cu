@@ -254,7 +254,9 @@ int32_t pstm::ctx::check_error_word(Ctx *c) {
     cudaError_t e = cudaMemcpy(&w, c->errword.ptr, sizeof(w), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(c, e, "reading the error word");
     if (w & KERR_WAIT_TIMEOUT)
-        return fail(c, PSTM_ERR_TIMEOUT, "a bounded wait for a trace-row copy gave up; the tile was not written");
+        return fail(c, PSTM_ERR_TIMEOUT,
+                    "a bounded wait for a trace-row copy gave up; the image and fold may hold partial sums "
+                    "of this call and must be discarded");
     return PSTM_OK;
 }
 

@@ -87,6 +87,9 @@ struct KParams {
     int32_t cr_k_zero;           // |k| < 1e-10: straight-ray fallback with v0
     int32_t compensated;
     int32_t *err;                // device error word (KernelError bits)
+    int32_t wait_iters;          // polls of one bounded mbarrier wait before it gives up
+    int32_t inject_stall;        // fault injection: the first chunks' copies are never issued, so the
+                                 // bounded waits for them run out (host-selected, tests only)
 };
 
 }  // namespace pstm

@@ -47,7 +47,7 @@ namespace pstm {
 constexpr int kThreads = 512;        // lanes per CTA = output times per r
 constexpr int kMaxChunk = 32;        // traces per chunk, upper bound
 constexpr int kGeoDoubles = 8;       // packed geometry per trace: sx sy rx ry mx my w 0
-constexpr int kWaitIters = 1 << 20;  // bound of every mbarrier wait loop
+constexpr int kWaitIters = 1 << 20;  // default bound of every mbarrier wait loop (KParams::wait_iters)
 
 // Unroll factors of the pair loops (records without / with a lane in the taper band).
 #ifndef PSTM_UNROLL_PLAIN
@@ -122,9 +122,10 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
-// Bounded wait for the mbarrier phase with the given parity; false = gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int i = 0; i < kWaitIters; ++i) {
+// Bounded wait for the mbarrier phase with the given parity: at most `iters`
+// polls (each a potentially blocking try_wait); false = gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int iters) {
+    for (int i = 0; i < iters; ++i) {
         uint32_t done;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
                      " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
@@ -596,14 +597,17 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     // chunk k of this item is the CTA's chunk g = chunk_base + k: buffer g & 1,
     // mbarrier phase parity (g >> 1) & 1
     const int b0 = (int)(chunk_base & 1);
-    if (tid == 0) {
+    const int wait_iters = P.wait_iters;
+    // (fault injection: with inject_stall the first copies are never issued, so
+    // nothing completes their phase and the bounded wait below runs out)
+    if (tid == 0 && !P.inject_stall) {
         if (chunk_base > 0) fence_proxy_async();   // the previous item's reads of the buffers
         if (n_chunks > 0) issue_chunk(0, b0);
         if (n_chunks > 1) issue_chunk(1, b0 ^ 1);
     }
     bool aborted = false;
     if (n_chunks > 0) {
-        const bool ok = mbar_wait(b0 ? bar1 : bar0, (uint32_t)((chunk_base >> 1) & 1));
+        const bool ok = mbar_wait(b0 ? bar1 : bar0, (uint32_t)((chunk_base >> 1) & 1), wait_iters);
         if (__syncthreads_or(!ok)) aborted = true;
         else build_records(0, b0);
     }
@@ -764,7 +768,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         bool timeout = false;
         if (k + 1 < n_chunks) {
             const int nb = buf ^ 1;
-            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1));
+            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1), wait_iters);
             if (!timeout) build_records(k + 1, nb);
         }
         if ((k + 1) % flush_every == 0) flush();
@@ -783,10 +787,10 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         // a copy never completed: report, drain what may still be in flight, leave
         if (tid == 0) {
             atomicOr(P.err, (int)KERR_WAIT_TIMEOUT);
-            mbar_wait(bar0, 0);
-            mbar_wait(bar0, 1);
-            mbar_wait(bar1, 0);
-            mbar_wait(bar1, 1);
+            mbar_wait(bar0, 0, wait_iters);
+            mbar_wait(bar0, 1, wait_iters);
+            mbar_wait(bar1, 0, wait_iters);
+            mbar_wait(bar1, 1, wait_iters);
         }
         __syncthreads();
         return false;

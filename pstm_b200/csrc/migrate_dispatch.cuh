@@ -2,30 +2,52 @@
 // kind is instantiated in its own translation unit (migrate_k<kind>.cu) so
 // that they compile in parallel.
 #pragma once
+#include <mutex>
+
 #include "launch.h"
 #include "migrate.cuh"
 
 namespace pstm {
 
+// Dynamic shared-memory opt-in of one kernel.  cudaFuncSetAttribute applies to
+// the calling thread's current device only, so the size set so far is kept per
+// device; the mutex orders host threads that launch concurrently.
+struct SmemOptIn {
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu;
+    size_t configured[kMaxDevices] = {};
+};
+
+template <typename Kernel>
+static cudaError_t opt_in_smem(SmemOptIn &state, Kernel kern, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;   // within the default limit
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= SmemOptIn::kMaxDevices)
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    std::lock_guard<std::mutex> lock(state.mu);
+    if (smem <= state.configured[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) state.configured[dev] = smem;
+    return e;
+}
+
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
 static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L) {
     if (!L.bins) {
         auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
-        static size_t configured = 0;   // dynamic shared memory opt-in, per instantiation
-        if (L.smem > configured) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
-            if (e != cudaSuccess) return e;
-            configured = L.smem;
-        }
+        static SmemOptIn opt_in;   // per instantiation
+        cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
+        if (e != cudaSuccess) return e;
         kern<<<L.grid, kThreads, L.smem, L.stream>>>(P, Pg);
         return cudaGetLastError();
     }
     auto kern = migrate_persistent_kernel<TT, AMP, VEL3D, EXACT, W2>;
-    static size_t configured = 0;
-    if (L.smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+    static SmemOptIn opt_in;
+    {
+        cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
         if (e != cudaSuccess) return e;
-        configured = L.smem;
     }
     unsigned ctas = L.grid.x;
     if (ctas == 0) {

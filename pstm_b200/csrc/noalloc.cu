@@ -17,6 +17,10 @@
 // accumulated with "+=".  All calls share the array and it keeps the last
 // call's contents, so calls whose work overlaps on the GPU (different streams,
 // different host threads) race and must be serialised by the caller.
+//
+// The kernel reports device-side failures (a bounded wait for a trace-row copy
+// that gave up) in an error word inside the array; pstm_cuda_noalloc_status
+// reads it back once the caller's stream has drained.
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <mutex>
@@ -178,5 +182,22 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     L.stream = st;
     e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, exact, L);
     if (e != cudaSuccess) return cuda_fail(e, "migrate kernel launch");
+    return PSTM_OK;
+}
+
+// Status of the last allocation-free call on the current device: waits for
+// `stream`, then reads the kernel's error word from the scratch array (a copy
+// from the array's symbol into a host int: nothing is allocated).
+extern "C" int32_t pstm_cuda_noalloc_status(void *stream) {
+    cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "waiting for the allocation-free call");
+    int32_t w = 0;
+    e = cudaMemcpyFromSymbol(&w, g_scratch, sizeof(w), kOffErr, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "reading the allocation-free error word");
+    if (w & KERR_WAIT_TIMEOUT)
+        return fail(PSTM_ERR_TIMEOUT,
+                    "a bounded wait for a trace-row copy gave up in the last allocation-free call; its image "
+                    "and fold may hold partial sums and must be discarded");
     return PSTM_OK;
 }

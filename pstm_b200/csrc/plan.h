@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "pstm_cuda.h"
@@ -131,6 +132,17 @@ inline KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *o
                        ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) &&
                         !P.cr_k_zero)) ? 1 : 0;
     P.compensated = prm->compensated ? 1 : 0;
+    P.wait_iters = kWaitIters;
+    // Fault injection for the tests of the bounded waits: PSTM_CUDA_INJECT_FAULT=wait
+    // leaves the first trace chunks' copies unissued, so the kernel's bounded
+    // wait for them runs out after a few polls and it reports KERR_WAIT_TIMEOUT.
+    // Read when a launch is prepared (a captured batch keeps what it saw).
+    if (const char *inj = std::getenv("PSTM_CUDA_INJECT_FAULT")) {
+        if (std::strcmp(inj, "wait") == 0) {
+            P.inject_stall = 1;
+            P.wait_iters = 256;
+        }
+    }
 
     // pillar patch: PB pillars as px x py, favouring y (the fastest image axis)
     int py = PB, px = 1;

@@ -516,12 +516,10 @@ int32_t pstm_cuda_surrogate_gradients(void *ctx, const pstm_surrogate *net, cons
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
     cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : c->stream;
-    static bool configured = false;
-    if (!configured) {
-        e = cudaFuncSetAttribute(train_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
-        if (e != cudaSuccess) return cuda_fail(c, e, "configuring the training kernel");
-        configured = true;
-    }
+    // set on every call: the attribute belongs to the current device, and a
+    // context may live on any device
+    e = cudaFuncSetAttribute(train_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+    if (e != cudaSuccess) return cuda_fail(c, e, "configuring the training kernel");
     const int blocks = (n + kTrainRows - 1) / kTrainRows;
     train_grad_kernel<<<blocks, 32 * kTrainWarps, sizeof(TrainSmem), st>>>(net->params, to_norm(net), raw, residual,
                                                                          n, 1.f / (float)n, grads, loss_sum);

@@ -259,7 +259,15 @@ class CudaKernel:
         return autotune_bins(self, traces, bins, geometry, velocity, config, kernel_type, pairs_per_candidate)
 
     def synchronize(self) -> None:
+        """Wait for this backend's work, then report device-side failures
+        (a bounded wait that gave up raises ``PstmCudaError`` with
+        ``ERR_TIMEOUT``).  Device-tensor calls run on torch's current stream,
+        so that device is synchronised first."""
         if self._ctx is not None:
+            import sys
+            torch = sys.modules.get("torch")
+            if torch is not None and torch.cuda.is_initialized():
+                torch.cuda.synchronize(self._device)
             nat.check(self._lib.pstm_cuda_synchronize(self._ctx), self._ctx, self._lib)
 
     def cleanup(self) -> None:

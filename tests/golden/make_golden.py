@@ -1,7 +1,7 @@
 """Generate golden fixtures by running the reference implementation.
 
 Run in a container where the reference project is importable (it is read
-from REF, default /root/reference); the tests read only its output.  Writes
+from REF: ``PSTM_REFERENCE``, default the installed reference in ``baseline/_ref``); the tests read only its output.  Writes
 ``*.npz`` next to this file:
 
 * ``numba_*.npz``   inputs and outputs of the reference's registered CPU
@@ -23,7 +23,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 

@@ -2,7 +2,7 @@
 (``pstm/algorithm/curved_ray.py:145-201``) on seeded v_rms(t) functions,
 including short axes and axes with fewer than two samples in the 500 ms
 window.  Writes ``tests/golden/gradient_from_vrms.npz``; run where the
-reference is at REF (default /root/reference):
+reference is at REF (``PSTM_REFERENCE``, default the installed reference in ``baseline/_ref``):
 
     PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_gradient_golden.py
 """
@@ -13,7 +13,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gradient_from_vrms.npz")
 
 

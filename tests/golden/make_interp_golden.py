@@ -4,7 +4,7 @@ Calls ``interpolate_sample`` of ``pstm/kernels/interpolation.py`` (Numba) from
 the reference checkout for every method on seeded traces and sample
 positions (including the trace ends, where the higher-order methods fall back
 to linear) and stores them in ``tests/golden/interp_methods.npz``.  Run once in
-a container that has the reference at REF (default /root/reference):
+a container that has the reference at REF (``PSTM_REFERENCE``, default the installed reference in ``baseline/_ref``):
 
     NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_interp_golden.py
 """
@@ -16,7 +16,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 HERE = os.path.dirname(os.path.abspath(__file__))
 # the reference's method codes (interpolation.py:293-301)
 METHODS = {"nearest": 0, "linear": 1, "cubic": 2, "sinc4": 3, "sinc8": 4, "sinc16": 5, "lanczos3": 6, "lanczos5": 7}

@@ -2,8 +2,8 @@
 
 Builds ``oracle/_ref/libpstm_metal_ref.so`` -- the shaders
 ``pstm/metal/shaders/pstm_migration.metal``, ``pstm_curved_ray.metal`` and
-``pstm_anisotropic_vti.metal`` of the reference at REF (default
-/root/reference), compiled unchanged as C++ by ``oracle/Makefile``'s ``ref``
+``pstm_anisotropic_vti.metal`` of the reference at REF (``PSTM_REFERENCE``,
+default the installed reference in ``baseline/_ref``), compiled unchanged as C++ by ``oracle/Makefile``'s ``ref``
 target -- runs its kernels and helpers on seeded inputs and writes their
 inputs and outputs to ``tests/golden/metal_kernels.npz``; every kernel runs in
 its scalar form and in its ``_simd`` form (the Metal backend's default).  Run it in a
@@ -28,7 +28,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "metal_kernels.npz")
 
 # one entry per kernel run: kind, velocity ("1d" | "3d"), grid ("axes" | "rotated"),

@@ -7,7 +7,7 @@ case-1 subset (250 traces cut to 300 samples, 3 x 3 pillars, 300 output
 times) -- trace weights, time-varying aperture, taper, spreading and
 obliquity, 2-D fold -- once per non-linear method, and stores inputs and
 outputs in ``tests/golden/interp_numba_kernel.npz``.  Run once in a container
-that has the reference at REF (default /root/reference):
+that has the reference at REF (``PSTM_REFERENCE``, default the installed reference in ``baseline/_ref``):
 
     NUMBA_CACHE_DIR=/tmp/numba PYTHONDONTWRITEBYTECODE=1 \\
         python tests/golden/make_numba_interp_golden.py
@@ -19,7 +19,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 OUT = os.path.join(HERE, "interp_numba_kernel.npz")

@@ -3,7 +3,7 @@
 Runs ``compute_time_windows`` of ``pstm/algorithm/time_variant.py`` (pure
 Python + SciPy PCHIP) from the reference checkout and stores the windows of a
 few tables and time ranges in ``tests/golden/time_windows.npz``.  Run once in a
-container that has the reference at REF (default /root/reference):
+container that has the reference at REF (``PSTM_REFERENCE``, default the installed reference in ``baseline/_ref``):
 
     python tests/golden/make_tv_golden.py
 """
@@ -15,7 +15,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 CASES = [

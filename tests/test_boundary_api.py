@@ -1,7 +1,7 @@
 """The drop-in boundary against the reference's own API (CPU).
 
 Where the reference tree is importable (``PSTM_REFERENCE``, default
-/root/reference; skipped elsewhere), its carriers (``pstm/kernels/base.py``:
+the installed reference in ``baseline/_ref``; skipped elsewhere), its carriers (``pstm/kernels/base.py``:
 TraceBlock, OutputTile, VelocitySlice, KernelConfig, KernelMetrics) must have
 every field here under the same name with the same default, its
 ``KernelCapability`` members must exist here, ``CudaKernel`` must provide every
@@ -17,7 +17,8 @@ import sys
 import numpy as np
 import pytest
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 
 
 @pytest.fixture(scope="module")

@@ -17,7 +17,8 @@ import pytest
 from conftest import rel_l2
 from oracle import oracle
 
-REF = os.environ.get("PSTM_REFERENCE", "/root/reference")
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.environ.get("PSTM_REFERENCE") or os.path.join(_REPO, "baseline", "_ref")
 HERE = os.path.dirname(os.path.abspath(__file__))
 # Numba caches compiled functions; keep that cache inside the repository's own pytest cache
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(os.path.dirname(HERE), ".pytest_cache", "numba"))

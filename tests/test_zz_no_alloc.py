@@ -5,7 +5,11 @@ keeps its scratch in a fixed array of the library.  The test calls it through
 the C ABI with device buffers the test itself allocates, and compares two calls
 in a row with the same two calls of the context-based entry point
 pstm_cuda_migrate_tile_dev: fold bit-exact, image within the plain-kernel
-tolerance (relative L2 <= 1e-5).  This file is collected last on purpose.
+tolerance (relative L2 <= 1e-5).  After every call it reads the device-side
+status back with pstm_cuda_noalloc_status, and one test makes a bounded
+wait of the kernel run out (PSTM_CUDA_INJECT_FAULT=wait leaves the first
+trace copies unissued) to check that the status reports it.  This file is
+collected last on purpose.
 """
 from __future__ import annotations
 
@@ -93,6 +97,7 @@ def test_noalloc_matches_context_entry_point_twice():
             rc = L.pstm_cuda_migrate_tile_noalloc(ctypes.byref(td), ctypes.byref(od_na), ctypes.byref(vd),
                                                   ctypes.byref(pr), ctypes.c_void_p(stream))
             nat.check(rc, None, L)
+            nat.check(L.pstm_cuda_noalloc_status(ctypes.c_void_p(stream)), None, L)
             torch.cuda.synchronize()
             if call == 1:   # the first call may load the module; the second must not move memory
                 assert torch.cuda.mem_get_info()[0] == free_before
@@ -123,3 +128,48 @@ def test_noalloc_rejects_inputs_beyond_its_scratch():
     assert rc == nat.ERR_INVALID_ARGUMENT
     assert b"131072" in L.pstm_cuda_last_error(None)
     assert float(img.abs().max()) == 0.0
+
+
+def test_noalloc_status_reports_a_wait_that_gave_up(monkeypatch):
+    """A bounded wait that runs out leaves PSTM_ERR_TIMEOUT in the status; the
+    next call clears it and matches the context entry point again."""
+    import torch
+    from pstm_b200 import build, workloads
+    from pstm_b200 import _native as nat
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    build.build()
+    L = nat.load()
+    torch.cuda.set_device(0)
+    case = workloads.config1(n_traces=2000, nx=8, ny=6, nt=500)
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    zeros = lambda shape, dt: torch.zeros(shape, dtype=dt, device="cuda")
+    td, vd, pr, axes, keep = _descs(case, dev)
+    shape = case.output.image.shape
+    stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+
+    od_bad, img_bad, fold_bad = _output(nat, shape, axes, zeros)
+    monkeypatch.setenv("PSTM_CUDA_INJECT_FAULT", "wait")
+    rc = L.pstm_cuda_migrate_tile_noalloc(ctypes.byref(td), ctypes.byref(od_bad), ctypes.byref(vd),
+                                          ctypes.byref(pr), ctypes.c_void_p(stream))
+    assert rc == nat.OK   # asynchronous: the launch itself succeeds
+    assert L.pstm_cuda_noalloc_status(ctypes.c_void_p(stream)) == nat.ERR_TIMEOUT
+    assert b"partial sums" in L.pstm_cuda_last_error(None)
+    monkeypatch.delenv("PSTM_CUDA_INJECT_FAULT")
+
+    od_na, img_na, fold_na = _output(nat, shape, axes, zeros)
+    od_ref, img_ref, fold_ref = _output(nat, shape, axes, zeros)
+    nat.check(L.pstm_cuda_migrate_tile_noalloc(ctypes.byref(td), ctypes.byref(od_na), ctypes.byref(vd),
+                                               ctypes.byref(pr), ctypes.c_void_p(stream)), None, L)
+    assert L.pstm_cuda_noalloc_status(ctypes.c_void_p(stream)) == nat.OK
+    ctx = ctypes.c_void_p()
+    nat.check(L.pstm_cuda_create(0, ctypes.byref(ctx)), None, L)
+    try:
+        nat.check(L.pstm_cuda_migrate_tile_dev(ctx, ctypes.byref(td), ctypes.byref(od_ref), ctypes.byref(vd),
+                                               ctypes.byref(pr), ctypes.c_void_p(stream)), ctx, L)
+        torch.cuda.synchronize()
+    finally:
+        L.pstm_cuda_destroy(ctx)
+    a, b = img_na.cpu().numpy(), img_ref.cpu().numpy()
+    np.testing.assert_array_equal(fold_na.cpu().numpy(), fold_ref.cpu().numpy())
+    assert np.linalg.norm(a - b) <= TOL * np.linalg.norm(b)
