@@ -208,6 +208,19 @@ int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *traces, const pst
  * discarded.  Each allocation-free call clears the word when it starts. */
 int32_t pstm_cuda_noalloc_status(void *stream);
 
+/* The precision form's trace format (no reference counterpart: the reference
+ * keeps FP32 traces, TraceBlock.amplitudes, pstm/kernels/base.py:27-116).
+ * Converts n_traces FP32 rows (src, src_stride elements apart) to FP16 rows
+ * (dst, dst_stride elements apart) with one power-of-two scale per trace --
+ * the trace times 2^e, its largest |amplitude| in [2^13, 2^14) -- and writes
+ * weights_out[i] = (weights ? weights[i] : 1) * 2^-e, so that migrating the
+ * FP16 panel with weights_out gives the FP32 panel's image up to the FP16
+ * rounding of the amplitudes.  Device pointers; asynchronous on `stream`
+ * (NULL = the context's stream). */
+int32_t pstm_cuda_traces_to_f16(void *ctx, const float *src, int64_t n_traces, int32_t n_samples,
+                                int64_t src_stride, void *dst, int64_t dst_stride, const double *weights,
+                                double *weights_out, void *stream);
+
 /* One output of the batched form: a contiguous range of the batch's traces and
  * its own image and fold.  Reference: one bin of the gather-bin loop,
  * pstm/pipeline/executor.py:960-975, which migrates every offset/OVT bin into

@@ -155,6 +155,8 @@ SIGNATURES = {
                                                             ctypes.POINTER(LearnedReport), _vp]),
     "pstm_cuda_interp_rows": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, ctypes.c_int32, _vp,
                                                ctypes.c_int32, _vp, _vp, _vp]),
+    "pstm_cuda_traces_to_f16": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, _vp,
+                                                 ctypes.c_int64, _vp, _vp, _vp]),
     "pstm_cuda_measure_sfu_peak": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "pstm_cuda_synchronize": (ctypes.c_int32, [_vp]),
     "pstm_cuda_last_error": (ctypes.c_char_p, [_vp]),

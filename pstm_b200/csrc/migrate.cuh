@@ -56,6 +56,11 @@ constexpr int kWaitIters = 1 << 20;  // default bound of every mbarrier wait loo
 #ifndef PSTM_UNROLL_TAPER
 #define PSTM_UNROLL_TAPER 2
 #endif
+// 1: the plain pair loop takes two records per step and does their weight
+// arithmetic with packed FP32 pairs (add/mul/fma.f32x2, sm_100)
+#ifndef PSTM_PACKED_PAIRS
+#define PSTM_PACKED_PAIRS 1
+#endif
 #define PSTM_PRAGMA_STR(x) #x
 #define PSTM_UNROLL(n) _Pragma(PSTM_PRAGMA_STR(unroll n))
 
@@ -390,6 +395,7 @@ struct CtaShared {
     int rank[kMaxPB][kMaxChunk];
     unsigned long long bar[2];
     long long item;
+    int unit[2];   // work-unit counters of the pair loop, by chunk parity
 };
 
 // Migrates one item.  `chunk_base` counts the chunks this CTA staged before
@@ -421,6 +427,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     float *const s_err = s_acc + PB * R * kThreads;   // [PB][R][kThreads] when comp
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kThreads / 32;
     const int pbx = it.pbx, pby = it.pby;
     __syncthreads();   // the previous item is done with the shared state
     if (tid < PB) {
@@ -433,7 +440,9 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         s_oy[tid] = ok ? (P.yg ? P.yg[p] : P.ya[iy]) : 0.0;
     }
     const uint32_t bar0 = smem_u32(&sh.bar[0]), bar1 = smem_u32(&sh.bar[1]);
-    const int t_lane = it.tblock * (kThreads * R) + tid;
+    const int t_base = it.tblock * (kThreads * R);
+    const int t_lane = t_base + tid;   // this thread's times (flush, fold): t_lane + r * kThreads
+    const int units_per_r = PB * kWarps, n_units = units_per_r * R;
 
     // hot-loop constants in registers
     const float s_scale = P.s_scale, s_offset = P.s_offset;
@@ -453,6 +462,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     const int flush_every = P.flush_every;
 
     for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
+    if (tid == 0) sh.unit[0] = sh.unit[1] = 0;
 
     // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
     // rows when they are 16-byte aligned) into buffer b
@@ -621,15 +631,31 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         const unsigned char *ampb = amp_base + buf * amp_bytes;
 
         // ---------------- pairs of chunk k
+        // Work units are (pillar, block of 32 output times); a warp takes the
+        // next unit from the CTA's counter for this chunk, deepest time blocks
+        // first.  Deep times have wide apertures and many records inside them,
+        // shallow ones few, so a fixed warp-to-time mapping leaves the warps
+        // with the shallow blocks idle at the chunk barrier.  A unit's partial
+        // sums stay where the fixed mapping keeps them (lane vt of the block).
+        if (tid == 0) sh.unit[(k + 1) & 1] = 0;   // the next chunk's counter: chunk k-1 is done with it
 #pragma unroll 1
-        for (int q = 0; q < PB; ++q) {
+        for (;;) {
+            int u = 0;
+            if (lane == 0) u = atomicAdd(&sh.unit[k & 1], 1);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (u >= n_units) break;
+            const int ur = u / units_per_r;           // 0 = the deepest r
+            const int uw = u - ur * units_per_r;
+            const int r = R - 1 - ur;
+            const int wb = kWarps - 1 - uw / PB;      // time block within r, deepest first
+            const int q = uw - (kWarps - 1 - wb) * PB;
             const int p = s_pid[q];
             if (p < 0) continue;
+            const int vt = wb * 32 + lane;            // the lane whose partial sums these are
             const float4 *A_q = recA + q * kMaxChunk;
             const float dl = A_q[lane].x;   // this lane's slot of the sorted distances
-#pragma unroll 1
-            for (int r = 0; r < R; ++r) {
-                const int t = t_lane + r * kThreads;
+            {
+                const int t = t_base + vt + r * kThreads;
                 TimeState ts;
                 PtState s;
                 load_states<TT, EXACT>(P, p, t, ts, s);
@@ -722,6 +748,76 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     }
                     return amp * (w * gw);
                 };
+                // The plain case (records inside every lane's aperture, no taper band,
+                // every T of the warp above 1 ms) two records at a time: the traveltime,
+                // sample index and amplitude reads per record, then the interpolation
+                // and the weights of both in packed FP32 pairs.  Same operations as
+                // `pair`; the AA weight is clamp(1 - u aa_k, L, H) with L = max(0,
+                // 1 - aaA), H = max(0, 1 - f_dom/500), the same function as
+                // max(0, 1 - max(min(u aa_k, aaA), f_dom/500)).
+                const float aa_lo = fmaxf(0.f, 1.f - s.aaA), aa_hi = fmaxf(0.f, 1.f - aa_cB);
+                auto front = [&](int c, float &a0, float &a1, float &f, float &T, float &w, float &mz) {
+                    const int ri = q * kMaxChunk + c;
+                    const float4 A = recA[ri];
+                    const int roff = __float_as_int(A.w);
+                    int i0;
+                    bool ok;
+                    if constexpr (EXACT) {
+                        const double2 B = reinterpret_cast<const double2 *>(recA + RECS)[ri];
+                        const double T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
+                        const double v = T2 + magic;
+                        const unsigned vh = (unsigned)__double2hiint(v), vl = (unsigned)__double2loint(v);
+                        const unsigned iu = __funnelshift_r(vl, vh, 21);
+                        ok = iu < ns_m1;
+                        i0 = ok ? (int)iu : 0;
+                        f = __uint_as_float(0x3F800000u | ((vl & 0x1FFFFFu) << 2));   // 1 + fraction
+                        T = double_to_float_trunc(T2);
+                    } else {
+                        const float4 B = reinterpret_cast<const float4 *>(recA + RECS)[ri];
+                        float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if constexpr (HAS_C) Cc = reinterpret_cast<const float4 *>(recA + 2 * RECS)[ri];
+                        T = traveltime<TT>(P, ts, s, B, Cc);
+                        if constexpr (TT != TT_STRAIGHT) T = ts.tz ? 0.f : T;
+                        float sidx = fmaf(T, s_scale, s_offset);
+                        const float x = fabsf(sidx - g_mid);
+                        const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
+                        const bool band = !fast_ok && !ts.tz && x <= g_out;
+                        if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
+                        ok = fast_ok;
+                        pmask |= band ? (1u << c) : 0u;
+                        sidx = ok ? sidx : 0.f;
+                        const float fl = __fadd_rd(sidx, 8388608.f);
+                        i0 = __float_as_int(fl) - 0x4B000000;
+                        f = sidx - (fl - 8388608.f);
+                    }
+                    const unsigned char *row = ampb + roff;
+                    a0 = amp_at<AMP>(row, i0);
+                    a1 = amp_at<AMP>(row, i0 + 1);
+                    w = ok ? A.y : 0.f;
+                    mz = A.z;
+                };
+                auto plain2 = [&](int c, float2 &acc) {
+                    float2 a0, a1, f, T, w, mz;
+                    front(c, a0.x, a1.x, f.x, T.x, w.x, mz.x);
+                    front(c + 1, a0.y, a1.y, f.y, T.y, w.y, mz.y);
+                    const float2 m1 = make_float2(-1.f, -1.f);
+                    if constexpr (EXACT) f = __fadd2_rn(f, m1);   // the fraction, exactly
+                    const float2 amp = __ffma2_rn(f, __ffma2_rn(a0, m1, a1), a0);
+                    const float2 rT = make_float2(rcp_approx(T.x), rcp_approx(T.y));
+                    const float2 K2 = make_float2(s.K, s.K);
+                    float2 g;
+                    if (W2 || w_two) g = __fmul2_rn(__fmul2_rn(K2, rT), rT);
+                    else if (w_one) g = __fmul2_rn(K2, rT);
+                    else g = make_float2(1.f, 1.f);
+                    if (aa_on) {
+                        const float2 u = __fmul2_rn(mz, rT);
+                        float2 y = __ffma2_rn(u, make_float2(-s.aa_k, -s.aa_k), make_float2(1.f, 1.f));
+                        y.x = u.x >= s.aa_thr ? fminf(fmaxf(y.x, aa_lo), aa_hi) : 1.f;
+                        y.y = u.y >= s.aa_thr ? fminf(fmaxf(y.y, aa_lo), aa_hi) : 1.f;
+                        g = __fmul2_rn(g, y);
+                    }
+                    acc = __ffma2_rn(amp, __fmul2_rn(w, g), acc);
+                };
                 using F = std::false_type;
                 using Tr = std::true_type;
                 float a = 0.f;
@@ -730,6 +826,13 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     if (small_t) {
                         PSTM_UNROLL(PSTM_UNROLL_TAPER)
                         for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, Tr{}, Tr{});
+                    } else if (PSTM_PACKED_PAIRS) {
+                        float2 acc = make_float2(0.f, 0.f);
+                        int c = 0;
+                        PSTM_UNROLL(2)
+                        for (; c + 1 < n0; c += 2) plain2(c, acc);
+                        if (c < n0) a += pair(c, F{}, F{}, F{}, F{}, Tr{});
+                        a += acc.x + acc.y;
                     } else {
                         PSTM_UNROLL(PSTM_UNROLL_PLAIN)
                         for (int c = 0; c < n0; ++c) a += pair(c, F{}, F{}, F{}, F{}, Tr{});
@@ -753,10 +856,10 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         a += pair(c, Tr{}, Tr{}, Tr{}, Tr{}, F{});
                     }
                 }
-                float &sa = s_acc[(q * R + r) * kThreads + tid];
+                float &sa = s_acc[(q * R + r) * kThreads + vt];
                 if (comp) {   // TwoSum: sa + a = t + e exactly; the errors are kept apart
                     const float s0 = sa, t = s0 + a, bp = t - s0;
-                    s_err[(q * R + r) * kThreads + tid] += (s0 - (t - bp)) + (a - bp);
+                    s_err[(q * R + r) * kThreads + vt] += (s0 - (t - bp)) + (a - bp);
                     sa = t;
                 } else {
                     sa += a;
@@ -771,10 +874,13 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1), wait_iters);
             if (!timeout) build_records(k + 1, nb);
         }
-        if ((k + 1) % flush_every == 0) flush();
         if (__syncthreads_or(timeout)) {   // also: buffer `buf` is free again
             aborted = true;
             break;
+        }
+        if ((k + 1) % flush_every == 0) {   // every unit of the chunk has added its sums
+            flush();
+            __syncthreads();               // before the next chunk's units add again
         }
         if (tid == 0 && k + 2 < n_chunks) {
             fence_proxy_async();

@@ -65,6 +65,19 @@ def float32_to_bf16_bits(a: np.ndarray) -> np.ndarray:
     return ((u + rounding) >> 16).astype(np.uint16)
 
 
+def scaled_f16(amps: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """FP32 traces -> (FP16 traces, per-trace 2^-e): the precision form's
+    format, the rule of ``pstm_cuda_traces_to_f16`` -- each trace times 2^e
+    with its largest |amplitude| in [2^13, 2^14), rounded to nearest even."""
+    a = np.asarray(amps, dtype=np.float32)
+    m = np.abs(a).max(axis=1) if a.shape[1] else np.zeros(a.shape[0], np.float32)
+    ok = (m > 0) & np.isfinite(m)
+    ex = np.frexp(np.where(ok, m, 1.0))[1]
+    e = np.where(ok, 14 - ex, 0).astype(np.int32)
+    out = (a * np.ldexp(np.float32(1.0), e)[:, None].astype(np.float32)).astype(np.float16)
+    return out, np.ldexp(1.0, -e)
+
+
 def bf16_bits_to_float32(b: np.ndarray) -> np.ndarray:
     return (np.asarray(b, dtype=np.uint16).astype(np.uint32) << 16).view(np.float32)
 
@@ -78,8 +91,10 @@ class CudaKernel:
         CUDA device index (default: ``PSTM_CUDA_DEVICE`` or 0).
     trace_dtype:
         ``"auto"`` keeps float32/float16 amplitudes as given and treats uint16
-        arrays as BF16 bit patterns; ``"bf16"``/``"f16"``/``"f32"`` convert on
-        the host first (the precision form stores traces in 16 bits).
+        arrays as BF16 bit patterns; ``"bf16"``/``"f16"``/``"f32"`` convert
+        host arrays first.  ``"f16"`` is the precision form: FP16 with one
+        power-of-two scale per trace carried by the trace weight
+        (:meth:`to_f16_panel`, which also converts device panels).
     compensated:
         TwoSum-compensated FP32 partial sums between the flushes into the
         image (``True``/``False``); ``"auto"`` compensates for 16-bit traces
@@ -398,7 +413,40 @@ class CudaKernel:
         keep.append(v)
         return v.ctypes.data, is3d, False
 
+    def to_f16_panel(self, traces):
+        """The precision form of a trace panel: a TraceBlock whose amplitudes
+        are FP16 with one power-of-two scale per trace and whose weights carry
+        the inverse scales (``pstm_cuda_traces_to_f16``; host arrays follow the
+        same rule in NumPy).  Geometry is shared with ``traces``."""
+        import dataclasses
+        amps = traces.amplitudes
+        w = getattr(traces, "weights", None)
+        if _is_torch_cuda(amps):
+            import torch
+            if amps.dtype != torch.float32 or amps.dim() != 2 or amps.stride(1) != 1:
+                raise ValueError("to_f16_panel takes (n_traces, n_samples) float32 CUDA amplitudes")
+            if self._ctx is None:
+                raise RuntimeError("Kernel not initialized")
+            n, ns = amps.shape
+            out = torch.empty((n, ns), dtype=torch.float16, device=amps.device)
+            wout = torch.empty((n,), dtype=torch.float64, device=amps.device)
+            win = None
+            if w is not None:
+                win = torch.as_tensor(w, dtype=torch.float64, device=amps.device).contiguous()
+            stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+            rc = self._lib.pstm_cuda_traces_to_f16(self._ctx, amps.data_ptr(), n, ns, amps.stride(0),
+                                                   out.data_ptr(), ns, win.data_ptr() if win is not None else None,
+                                                   wout.data_ptr(), ctypes.c_void_p(stream))
+            nat.check(rc, self._ctx, self._lib)
+            return dataclasses.replace(traces, amplitudes=out, weights=wout)
+        a16, inv = scaled_f16(np.asarray(amps, np.float32))
+        w = inv if w is None else np.asarray(w, np.float64) * inv
+        return dataclasses.replace(traces, amplitudes=a16, weights=w)
+
     def _trace_desc(self, traces, keep: list, devs: list) -> nat.TracesDesc:
+        if self._trace_dtype == "f16" and not _is_torch_cuda(traces.amplitudes) \
+                and np.asarray(traces.amplitudes).dtype != np.float16:
+            traces = self.to_f16_panel(traces)   # the precision form: per-trace scaled FP16
         amp_ptr, amp_code, amp_stride, amp_dev = self._amplitudes(traces.amplitudes, keep)
         td = nat.TracesDesc()
         td.amplitudes = amp_ptr

@@ -217,3 +217,38 @@ def test_bins_split_into_trace_segments(cuda_kernel_factory, monkeypatch):
         ref_img, ref_fold = _per_tile(k_ref, dtb, geo, dvel, cfg, "straight_ray", b0, n, shape)
         np.testing.assert_array_equal(folds[i].cpu().numpy(), ref_fold)
         assert rel_l2(imgs[i].cpu().numpy(), ref_img) <= 1e-6
+
+
+@pytest.mark.parametrize("kind", ["straight_ray", "anisotropic_vti"])
+def test_autotuned_segmented_batch_vs_fp64_oracle(kind, cuda_kernel_factory, monkeypatch):
+    """The whole composite path -- autotuned launch shape, bins split into
+    1 MiB trace segments with atomic adds, one graph-replayed persistent
+    launch -- against the FP64 oracle bin by bin: fold bit-exact, image within
+    the kind's tolerance."""
+    import torch
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, create_trace_block
+    from pstm_b200.cuda_kernel import Bin
+    counts = [2600, 400, 1900, 30]
+    bs, tb, dtb, out, vel, geo, dvel, cfg = _batch(counts, nx=20, ny=16, nt=400, ns=400, seed=51, kind=kind)
+    monkeypatch.setenv("PSTM_CUDA_SEGMENT_MB", "1")
+    k = cuda_kernel_factory(cfg)
+    shape = out.image.shape
+    imgs, folds = _outputs(len(counts), shape)
+    bins = [Bin(b0, n, imgs[i], folds[i]) for i, (b0, n) in enumerate(zip(bs.starts, bs.counts))]
+    k.autotune_bins(dtb, bins, geo, dvel, cfg, kernel_type=kind, pairs_per_candidate=1 << 29)
+    k.migrate_bins(dtb, bins, geo, dvel, cfg, kernel_type=kind)
+    torch.cuda.synchronize()
+    k.synchronize()
+    ocfg = cfg if kind == "straight_ray" else \
+        workloads.survey_config(kernel_type=kind, aa=True, eta=workloads.survey_eta(out.t_axis_ms))
+    tol = PLAIN_TOL if kind == "straight_ray" else KIND_TOL
+    for i, (b0, n) in enumerate(zip(bs.starts, bs.counts)):
+        sl = slice(int(b0), int(b0 + n))
+        sub = create_trace_block(tb.amplitudes[sl], tb.source_x[sl], tb.source_y[sl], tb.receiver_x[sl],
+                                 tb.receiver_y[sl], sample_rate_ms=tb.sample_rate_ms)
+        ref = OutputTile(image=np.zeros(shape), fold=np.zeros(shape, np.int32), x_axis=out.x_axis,
+                         y_axis=out.y_axis, t_axis_ms=out.t_axis_ms)
+        oracle.migrate(sub, ref, vel, ocfg, kind=kind)
+        np.testing.assert_array_equal(folds[i].cpu().numpy(), ref.fold)
+        assert rel_l2(imgs[i].cpu().numpy(), ref.image) <= tol, (i, kind)

@@ -47,3 +47,10 @@ def test_tiled_grid_equals_one_call(cuda_kernel_factory):
     np.testing.assert_array_equal(fold.cpu().numpy(), ref.fold.cpu().numpy())
     assert rel_l2(img.cpu().numpy(), ref.image.cpu().numpy()) <= 1e-6
     assert float(ref.image.abs().max()) > 0
+    # the tiled grid against the FP64 oracle directly: fold bit-exact, image <= 1e-5
+    from oracle import oracle
+    oref = OutputTile(image=np.zeros(full.image.shape), fold=np.zeros(full.fold.shape, np.int32),
+                      x_axis=full.x_axis, y_axis=full.y_axis, t_axis_ms=full.t_axis_ms)
+    oracle.migrate(tb, oref, vel, cfg)
+    np.testing.assert_array_equal(fold.cpu().numpy(), oref.fold)
+    assert rel_l2(img.cpu().numpy(), oref.image) <= 1e-5

@@ -76,6 +76,23 @@ def test_runs_equal_gathered_panel(kind, seg_mb, cuda_kernel_factory, monkeypatc
     np.testing.assert_array_equal(got.fold.cpu().numpy(), ref.fold.cpu().numpy())
     assert float(ref.image.abs().max()) > 0
     assert rel_l2(got.image.cpu().numpy(), ref.image.cpu().numpy()) <= 1e-6
+    # the runs against the FP64 oracle on the same traces directly
+    from oracle import oracle
+    from pstm_b200 import workloads
+    from pstm_b200.base import OutputTile, create_trace_block
+    ii = idx.cpu().numpy()
+    tb = case.traces
+    sub = create_trace_block(tb.amplitudes[ii], tb.source_x[ii], tb.source_y[ii], tb.receiver_x[ii],
+                             tb.receiver_y[ii], sample_rate_ms=tb.sample_rate_ms,
+                             weights=np.linspace(0.5, 1.5, tb.n_traces)[ii])
+    o = case.output
+    oref = OutputTile(image=np.zeros(o.image.shape), fold=np.zeros(o.fold.shape, np.int32), x_axis=o.x_axis,
+                      y_axis=o.y_axis, t_axis_ms=o.t_axis_ms)
+    ocfg = cfg if kind == "straight_ray" else \
+        workloads.survey_config(kernel_type=kind, aa=True, eta=workloads.survey_eta(o.t_axis_ms))
+    oracle.migrate(sub, oref, case.velocity, ocfg, kind=kind)
+    np.testing.assert_array_equal(got.fold.cpu().numpy(), oref.fold)
+    assert rel_l2(got.image.cpu().numpy(), oref.image) <= (1e-5 if kind == "straight_ray" else 1e-4)
 
 
 def test_single_run_no_runs_and_invalid_runs(cuda_kernel_factory):
