@@ -167,6 +167,26 @@ int32_t pstm_cuda_migrate_tile_runs_dev(void *ctx, const pstm_traces_desc *trace
                                         const pstm_velocity_desc *velocity, const pstm_params *params,
                                         void *stream);
 
+/* The trace-centric (scatter) schedule of a migration: instead of every tile
+ * reading every trace of its selection box, every trace is read for the whole
+ * output grid once.  The panel is cut into segments of segment_traces traces
+ * (0: 64 staged chunks; midpoint order, pstm_b200.spatial, keeps segments
+ * compact); on the device, each segment's midpoint box grown by the maximum
+ * aperture is mapped to pillar blocks by binary search in the ascending grid
+ * axes, the item counts are prefix-summed, and one persistent launch
+ * migrates (segment, pillar block, time block) items with FP32 partial sums
+ * per chunk and one atomic add per output sample per item.  Same result as
+ * pstm_cuda_migrate_tile_dev up to the order of floating-point additions;
+ * regular grids (x_axis, y_axis) and linear interpolation only.  Device
+ * pointers; asynchronous on `stream`, except that a non-null n_items_out
+ * synchronises it to report the number of items.  Replaces the reference's
+ * trace-centric kernel, pstm/metal/shaders/pstm_trace_centric.metal:112-236
+ * (one thread per trace, one atomic add per pair, a per-sample fold: here the
+ * fold is the Numba count of traces within the maximum aperture). */
+int32_t pstm_cuda_migrate_scatter_dev(void *ctx, const pstm_traces_desc *traces, int64_t segment_traces,
+                                      const pstm_output_desc *output, const pstm_velocity_desc *velocity,
+                                      const pstm_params *params, int64_t *n_items_out, void *stream);
+
 /* Same, host pointers: inputs are copied to the device, the tile is migrated
  * and image/fold are copied back and accumulated (+=) into the host arrays.
  * Synchronous, like the reference backends.  Native precedent: the pybind11

@@ -129,6 +129,9 @@ SIGNATURES = {
     "pstm_cuda_migrate_tile_runs_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(ctypes.c_int64),
                                                          ctypes.c_int32, ctypes.POINTER(OutputDesc),
                                                          ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params), _vp]),
+    "pstm_cuda_migrate_scatter_dev": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.c_int64,
+                                                       ctypes.POINTER(OutputDesc), ctypes.POINTER(VelocityDesc),
+                                                       ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_int64), _vp]),
     "pstm_cuda_migrate_tile_host": (ctypes.c_int32, [_vp, ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),
                                                      ctypes.POINTER(VelocityDesc), ctypes.POINTER(Params)]),
     "pstm_cuda_migrate_tile_noalloc": (ctypes.c_int32, [ctypes.POINTER(TracesDesc), ctypes.POINTER(OutputDesc),

@@ -129,7 +129,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     bp.tt = prm->traveltime;
     bp.amp = tr->amp_dtype;
     bp.per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
-    bp.exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
+    bp.exact = prm->precision == PSTM_PREC_EXACT;
     P.exact_units = bp.exact ? 1 : 0;
     P.curved_kind = (prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) ? 1 : 0;
     bp.n_p = bp.per_pillar ? (int64_t)out->nx * out->ny : 1;
@@ -139,6 +139,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
         (e = ensure(c->btab, n_tab * sizeof(double))) != cudaSuccess ||
         (e = ensure(c->ttime, (size_t)out->nt * 2 * sizeof(float4))) != cudaSuccess ||
         (e = ensure(c->ttimeA, (size_t)out->nt * sizeof(double))) != cudaSuccess ||
+        (e = ensure(c->ttimeV, (size_t)out->nt * sizeof(double))) != cudaSuccess ||
         (e = ensure(c->errword, sizeof(int32_t))) != cudaSuccess ||
         (e = ensure(c->kparams, sizeof(KParams))) != cudaSuccess ||
         (e = ensure(c->packed_geo, (size_t)tr->n_traces * kGeoDoubles * sizeof(double))) != cudaSuccess ||
@@ -149,6 +150,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     P.btab = reinterpret_cast<const double *>(c->btab.ptr);
     P.ttime = reinterpret_cast<const float4 *>(c->ttime.ptr);
     P.ttimeA = reinterpret_cast<const double *>(c->ttimeA.ptr);
+    P.ttimeV = reinterpret_cast<const double *>(c->ttimeV.ptr);
     P.geo = reinterpret_cast<const double *>(c->packed_geo.ptr);
     P.err = reinterpret_cast<int32_t *>(c->errword.ptr);
     size_t smem = 0;
@@ -212,7 +214,8 @@ int32_t enqueue_batch(Ctx *c, BatchPlan &bp, cudaStream_t st) {
     prep_time_table<<<blocks, 256, 0, st>>>(P, bp.n_p, reinterpret_cast<float4 *>(c->ttab.ptr),
                                             reinterpret_cast<double *>(c->btab.ptr),
                                             reinterpret_cast<float4 *>(c->ttime.ptr),
-                                            reinterpret_cast<double *>(c->ttimeA.ptr));
+                                            reinterpret_cast<double *>(c->ttimeA.ptr),
+                                            reinterpret_cast<double *>(c->ttimeV.ptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(c, e, "prep_time_table launch");
     blocks = (int)std::min<int64_t>((P.n_traces + 255) / 256, 148 * 32);
     if (blocks > 0) {

@@ -106,23 +106,26 @@ int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc 
         (e = ensure(c->btab, n_tab * sizeof(double))) != cudaSuccess ||
         (e = ensure(c->ttime, (size_t)out->nt * 2 * sizeof(float4))) != cudaSuccess ||
         (e = ensure(c->ttimeA, (size_t)out->nt * sizeof(double))) != cudaSuccess ||
+        (e = ensure(c->ttimeV, (size_t)out->nt * sizeof(double))) != cudaSuccess ||
         (e = ensure(c->errword, sizeof(int32_t))) != cudaSuccess)
         return cuda_fail(c, e, "allocating the per-time tables");
     float4 *tab = reinterpret_cast<float4 *>(c->ttab.ptr);
     double *btab = reinterpret_cast<double *>(c->btab.ptr);
-    const bool exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
+    const bool exact = prm->precision == PSTM_PREC_EXACT;
     P.exact_units = exact ? 1 : 0;
     P.curved_kind = (prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) ? 1 : 0;
     {
         int blocks = (int)(((int64_t)n_tab + 255) / 256);
         if (blocks > 148 * 32) blocks = 148 * 32;
         prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, tab, btab, reinterpret_cast<float4 *>(c->ttime.ptr),
-                                                reinterpret_cast<double *>(c->ttimeA.ptr));
+                                                reinterpret_cast<double *>(c->ttimeA.ptr),
+                                                reinterpret_cast<double *>(c->ttimeV.ptr));
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(c, e, "prep_time_table launch");
     }
     P.ttime = reinterpret_cast<const float4 *>(c->ttime.ptr);
     P.ttimeA = reinterpret_cast<const double *>(c->ttimeA.ptr);
+    P.ttimeV = reinterpret_cast<const double *>(c->ttimeV.ptr);
     P.ttab = tab;
     P.btab = btab;
     P.err = reinterpret_cast<int32_t *>(c->errword.ptr);
@@ -253,6 +256,10 @@ int32_t pstm::ctx::check_error_word(Ctx *c) {
     int32_t w = 0;
     cudaError_t e = cudaMemcpy(&w, c->errword.ptr, sizeof(w), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(c, e, "reading the error word");
+    if (w & KERR_UNSORTED_AXIS)
+        return fail(c, PSTM_ERR_INVALID_ARGUMENT,
+                    "the scatter schedule needs ascending x and y axes; the image and fold were not computed "
+                    "correctly and must be discarded");
     if (w & KERR_WAIT_TIMEOUT)
         return fail(c, PSTM_ERR_TIMEOUT,
                     "a bounded wait for a trace-row copy gave up; the image and fold may hold partial sums "
@@ -323,6 +330,7 @@ void pstm_cuda_destroy(void *ctx) {
     release(c->btab);
     release(c->ttime);
     release(c->ttimeA);
+    release(c->ttimeV);
     release(c->kparams);
     release(c->errword);
     release(c->packed_geo);
@@ -330,6 +338,7 @@ void pstm_cuda_destroy(void *ctx) {
     for (auto &g : c->geo) release(g);
     release(c->xa); release(c->ya); release(c->xg); release(c->yg); release(c->ta);
     release(c->vel); release(c->eta); release(c->image); release(c->fold);
+    release(c->scatter_ends);
     release_batch(c);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

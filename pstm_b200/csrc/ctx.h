@@ -29,7 +29,7 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    DevBuf ttab, btab, ttime, ttimeA, kparams, errword, packed_geo;
+    DevBuf ttab, btab, ttime, ttimeA, ttimeV, kparams, errword, packed_geo;
     // staging for the host-pointer path
     DevBuf amps, geo[7], xa, ya, xg, yg, ta, vel, eta, image, fold;
     int force_r = 0;      // PSTM_CUDA_R override of the output times per lane
@@ -39,6 +39,7 @@ struct Ctx {
     DevBuf bins, counter, tune_image, tune_fold;
     DevBuf probe;                           // learned form: per-probe residuals
     DevBuf seg_bins, seg_counter;           // per-tile launches split into trace segments
+    DevBuf scatter_ends;                    // scatter schedule: prefix counts of the segments' items
     int64_t segment_bytes = 24ll << 20;     // trace-panel bytes per segment (0: never split)
     std::vector<unsigned char> graph_key;   // arguments the cached graph was captured with
     cudaGraphExec_t graph = nullptr;

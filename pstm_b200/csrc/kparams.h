@@ -10,7 +10,7 @@ enum AmpKind { AMP_F32 = 0, AMP_BF16 = 1, AMP_F16 = 2 };
 enum TTKind { TT_STRAIGHT = 0, TT_CURVED = 1, TT_VTI = 2, TT_CURVED_VTI = 3 };
 
 // error bits a kernel can raise in *err
-enum KernelError { KERR_WAIT_TIMEOUT = 1 };
+enum KernelError { KERR_WAIT_TIMEOUT = 1, KERR_UNSORTED_AXIS = 2 };
 
 // One output of the persistent form: its traces and its image/fold.
 struct BinWork {
@@ -18,6 +18,21 @@ struct BinWork {
     int64_t n_traces;
     void *image;
     int32_t *fold;
+};
+
+// The scatter schedule of the persistent form: the panel cut into segments
+// of seg_traces traces; segment s reaches the pillar blocks
+// [pbx0, pbx1] x [pby0, pby1] (empty when pbx0 > pbx1) and contributes
+// (pbx1 - pbx0 + 1) (pby1 - pby0 + 1) n_tblk work items; ends[s] is the
+// inclusive prefix sum of those counts.
+struct SegmentBox {
+    int32_t pbx0, pbx1, pby0, pby1;
+};
+struct ScatterWork {
+    const SegmentBox *boxes;
+    const long long *ends;
+    int64_t n_seg;
+    int64_t seg_traces;
 };
 
 struct KParams {
@@ -87,6 +102,11 @@ struct KParams {
     int32_t cr_k_zero;           // |k| < 1e-10: straight-ray fallback with v0
     int32_t compensated;
     int32_t *err;                // device error word (KernelError bits)
+    // FP64 sample-index path of the curved kinds (samples as the time unit)
+    const double *ttimeV;        // per t: v(z) of the image depth, FP64 (curved kinds)
+    double cr_B0;                // 1 / (v0 dt)^2: |k| ~ 0 straight rays in v0
+    double cr_k2;                // k^2
+    double cr_inv_k_dt;          // 1 / (k dt)
     int32_t wait_iters;          // polls of one bounded mbarrier wait before it gives up
     int32_t inject_stall;        // fault injection: the first chunks' copies are never issued, so the
                                  // bounded waits for them run out (host-selected, tests only)

@@ -9,9 +9,10 @@
 
 namespace pstm {
 
-// One launch: the per-tile grid form (bins == nullptr: grid is (pillar
-// blocks, time blocks)) or the persistent form over `n_bins` outputs (grid.x
-// CTAs; grid.x == 0 asks for one CTA per SM times the occupancy).
+// One launch: the per-tile grid form (bins and items null: grid is (pillar
+// blocks, time blocks)), the persistent form over `n_bins` outputs, or the
+// persistent form over the segments of the scatter schedule (grid.x CTAs; grid.x == 0 asks
+// for one CTA per SM times the occupancy).
 struct Launch {
     dim3 grid = dim3(0, 1, 1);   // dim3's own default is (1, 1, 1)
     size_t smem = 0;
@@ -19,6 +20,8 @@ struct Launch {
     const BinWork *bins = nullptr;
     int n_bins = 0;
     unsigned long long *counter = nullptr;
+    // the scatter schedule instead of bins (persistent form; item count read on the device)
+    ScatterWork scatter = {nullptr, nullptr, 0, 0};
     bool configure_only = false;   // persistent form: set the shared-memory opt-in,
     unsigned *ctas_out = nullptr;  // report the CTA count and launch nothing
 };
@@ -34,20 +37,20 @@ extern template cudaError_t launch_migrate<TT_VTI>(const KParams &, const KParam
 extern template cudaError_t launch_migrate<TT_CURVED_VTI>(const KParams &, const KParams *, int, bool, bool,
                                                           const Launch &);
 
-// exact selects the FP64 sample-index path (straight rays only).
+// exact selects the FP64 sample-index path.
 inline cudaError_t launch_kind(int traveltime, const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact,
                                const Launch &L) {
     switch (traveltime) {
     case PSTM_TT_STRAIGHT: return launch_migrate<TT_STRAIGHT>(P, Pg, amp, vel3d, exact, L);
-    case PSTM_TT_CURVED: return launch_migrate<TT_CURVED>(P, Pg, amp, vel3d, false, L);
-    case PSTM_TT_VTI: return launch_migrate<TT_VTI>(P, Pg, amp, vel3d, false, L);
-    default: return launch_migrate<TT_CURVED_VTI>(P, Pg, amp, vel3d, false, L);
+    case PSTM_TT_CURVED: return launch_migrate<TT_CURVED>(P, Pg, amp, vel3d, exact, L);
+    case PSTM_TT_VTI: return launch_migrate<TT_VTI>(P, Pg, amp, vel3d, exact, L);
+    default: return launch_migrate<TT_CURVED_VTI>(P, Pg, amp, vel3d, exact, L);
     }
 }
 
 __global__ void pack_geometry(const KParams P, double *geo);
 __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
-                                double *ttimeA);
+                                double *ttimeA, double *ttimeV);
 __global__ void store_params(const KParams P, KParams *dst);
 
 // Work descriptors carried by value into store_bins (kernel parameters are

@@ -89,6 +89,12 @@ __device__ __forceinline__ double sqrt_newton(double q) {
     const double c = fma(-u, u, q);
     return fma(c, 0.5 * h, u);
 }
+// 1/x for x > 0: the hardware's approximate reciprocal refined by one Newton step.
+__device__ __forceinline__ double rcp_newton(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return fma(r, fma(-x, r, 1.0), r);
+}
 // Positive double in the float normal range -> float, truncating the
 // mantissa (|error| < 1 float ulp), with integer ops only.
 __device__ __forceinline__ float double_to_float_trunc(double x) {
@@ -151,6 +157,7 @@ struct TimeState {
     bool tzero;
     bool tz, tz_in;        // t0 = 0 with T = 0 exactly for every pair; its sample index inside the trace
     double A;              // EXACT: (t0 / (2 dt))^2 (at least 1e-20)
+    double vz64, vz2_64;   // EXACT, curved kinds: v(z) of the image depth and its square
 };
 
 // Quantities that depend on (pillar, time).
@@ -161,7 +168,9 @@ struct PtState {
     float aaA;             // 4 max(dx,dy) f_dom / v_w (AA)
     float aa_k, aa_thr;    // aaA / v_w per unit of T; minf / T above which sin(theta) >= 0.01
     float t02v2, c1, e2;   // VTI: (t0/2)^2 v^2, 1+2eta, 2 eta / v^2
+    float iv2r;            // 1/v_rms^2 (the curved+VTI ratio's hyperbolic leg; iv2 may be 1/v0^2)
     double B;              // EXACT: 1/(v dt)^2
+    double c1B, e2B2;      // EXACT, VTI kinds: (1+2eta) / (v dt)^2, 2 eta / (v dt)^4
 };
 
 template <int TT, bool EXACT>
@@ -180,9 +189,15 @@ __device__ __forceinline__ void load_states(const KParams &P, int p, int t, Time
     ts.tz = b.w >= 2.f;
     ts.tz_in = b.w == 2.f;
     ts.A = EXACT ? P.ttimeA[tc] : 0.0;
+    ts.vz64 = ts.vz2_64 = 0.0;
+    if constexpr (EXACT && (TT == TT_CURVED || TT == TT_CURVED_VTI)) {
+        ts.vz64 = P.ttimeV[tc];
+        ts.vz2_64 = ts.vz64 * ts.vz64;
+    }
     const int64_t ti = (P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc;
     const float4 tab = P.ttab[ti];
     s.iv2 = tab.x;
+    s.iv2r = tab.x;
     s.ap = valid ? tab.y : -1.f;   // a time past the tile end is never inside the aperture
     const float width = tab.y * P.taper_f;
     if (width > 0.f) {
@@ -213,6 +228,56 @@ __device__ __forceinline__ void load_states(const KParams &P, int p, int t, Time
         s.e2 = 2.f * tab.w * tab.x;
     }
     s.B = EXACT ? P.btab[ti] : 0.0;
+    s.c1B = s.e2B2 = 0.0;
+    if constexpr (EXACT && (TT == TT_VTI || TT == TT_CURVED_VTI)) {
+        double eta = P.eta_const;
+        if (P.eta) eta = P.eta3d ? P.eta[(int64_t)p * P.nt + tc] : P.eta[tc];
+        s.c1B = (1.0 + 2.0 * eta) * s.B;
+        s.e2B2 = 2.0 * eta * s.B * s.B;
+    }
+}
+
+// FP64 traveltime in samples (the EXACT path of the curved and VTI kinds) of
+// one pair from its record: B = {ds2, dr2}, C = curved {1/(bs br), 0} or
+// curved+VTI {1/bs, 1/br}, bs = v0 + sqrt(v0^2 + k^2 ds2).  The formulas of
+// traveltime_fp64 with every time divided by dt: A = (t0/2)^2/dt^2,
+// h^2/(v dt)^2 = h^2 B, and the VTI correction 2 eta h^4 / (v^2 (t0h^2 v^2 +
+// (1+2eta) h^2)) / dt^2 = e2B2 h^4 / (A + c1B h^2).
+template <int TT>
+__device__ __forceinline__ double exact_time_samples(const KParams &P, const TimeState &ts, const PtState &s,
+                                                     const double2 &B, const double2 &C) {
+    if constexpr (TT == TT_VTI) {
+        if (ts.tz) return 0.0;   // the reference's VTI leg is 0 at t0 = 0
+        const double Ds = fma(B.x, s.c1B, ts.A), Dr = fma(B.y, s.c1B, ts.A);
+        const double rr = rcp_newton(Ds * Dr);
+        const double qs = fma(-(s.e2B2 * B.x * B.x), Dr * rr, fma(B.x, s.B, ts.A));
+        const double qr = fma(-(s.e2B2 * B.y * B.y), Ds * rr, fma(B.y, s.B, ts.A));
+        return sqrt_newton(fmax(qs, 1e-300)) + sqrt_newton(fmax(qr, 1e-300));
+    } else if constexpr (TT == TT_CURVED) {   // |k| ~ 0: straight rays in v0 (curved_ray.py:35-38)
+        if (P.cr_k_zero) return sqrt_newton(fma(B.x, P.cr_B0, ts.A)) + sqrt_newton(fma(B.y, P.cr_B0, ts.A));
+        if (ts.tz) return 0.0;   // depth 0: both legs are log(1) = 0
+        const double as = ts.vz64 + sqrt_newton(fma(P.cr_k2, B.x, ts.vz2_64));
+        const double ar = ts.vz64 + sqrt_newton(fma(P.cr_k2, B.y, ts.vz2_64));
+        return log(as * ar * C.x) * P.cr_inv_k_dt;
+    } else {
+        double tcs, tcr;
+        if (P.cr_k_zero) {
+            tcs = sqrt_newton(fma(B.x, P.cr_B0, ts.A));
+            tcr = sqrt_newton(fma(B.y, P.cr_B0, ts.A));
+        } else {
+            if (ts.tz) return 0.0;
+            tcs = log((ts.vz64 + sqrt_newton(fma(P.cr_k2, B.x, ts.vz2_64))) * C.x) * P.cr_inv_k_dt;
+            tcr = log((ts.vz64 + sqrt_newton(fma(P.cr_k2, B.y, ts.vz2_64))) * C.y) * P.cr_inv_k_dt;
+        }
+        if (ts.tzero) return tcs + tcr;   // t0 = 0: the curved legs alone
+        // leg = t_curved sqrt(1 - corr / (A + h^2 B)), corr = e2B2 h^4 / (A + c1B h^2)
+        const double Hs = fma(B.x, s.B, ts.A), Hr = fma(B.y, s.B, ts.A);
+        const double Ds = fma(B.x, s.c1B, ts.A), Dr = fma(B.y, s.c1B, ts.A);
+        const double ps = Ds * Hs, pr = Dr * Hr;
+        const double rr = rcp_newton(ps * pr);
+        const double xs = s.e2B2 * B.x * B.x * (pr * rr), xr = s.e2B2 * B.y * B.y * (ps * rr);
+        return tcs * sqrt_newton(fmax(1.0 - xs, 1e-300)) + tcr * sqrt_newton(fmax(1.0 - xr, 1e-300));
+    }
 }
 
 // 0.5 (1 + cos(pi x)) = cos^2(pi x / 2) for x in [0, 1]: Taylor series of cos
@@ -346,8 +411,8 @@ __device__ __forceinline__ float traveltime(const KParams &P, const TimeState &t
             tcr = P.cr_inv_k_ln2 * lg2_approx(b * Cc.y);
         }
         if (ts.tzero) return tcs + tcr;
-        // leg = t_curved * sqrt(1 - corr / (t0h^2 + h^2/v^2)), corr = e2 h^4 / D
-        const float Hs = fmaf(B.x, s.iv2, ts.t0h2), Hr = fmaf(B.y, s.iv2, ts.t0h2);
+        // leg = t_curved * sqrt(1 - corr / (t0h^2 + h^2/v^2)), corr = e2 h^4 / D, v = v_rms
+        const float Hs = fmaf(B.x, s.iv2r, ts.t0h2), Hr = fmaf(B.y, s.iv2r, ts.t0h2);
         const float Ds = fmaf(s.c1, B.x, s.t02v2), Dr = fmaf(s.c1, B.y, s.t02v2);
         const float ps_ = Ds * Hs, pr_ = Dr * Hr;
         const float rr = rcp_approx(ps_ * pr_);
@@ -519,7 +584,14 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         const double br = v0 + sqrt(v0 * v0 + k2 * dr2);
                         Bf.z = (float)(k2 * ds2);
                         Bf.w = (float)(k2 * dr2);
-                        if constexpr (TT == TT_CURVED) {
+                        if constexpr (EXACT) {   // the C slot holds FP64 {1/(bs br), 0} or {1/bs, 1/br}
+                            const double2 c64 = TT == TT_CURVED ? make_double2(1.0 / (bs * br), 0.0)
+                                                                : make_double2(1.0 / bs, 1.0 / br);
+                            Cc = make_float4(__int_as_float(__double2loint(c64.x)),
+                                             __int_as_float(__double2hiint(c64.x)),
+                                             __int_as_float(__double2loint(c64.y)),
+                                             __int_as_float(__double2hiint(c64.y)));
+                        } else if constexpr (TT == TT_CURVED) {
                             Cc = make_float4((float)(1.0 / (bs * br)), 0.f, 0.f, 0.f);
                         } else {
                             Cc = make_float4((float)(1.0 / bs), (float)(1.0 / br), (float)(ds2 * ds2),
@@ -692,7 +764,14 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     bool ok;
                     if constexpr (EXACT) {
                         const double2 B = reinterpret_cast<const double2 *>(recA + RECS)[ri];
-                        const double T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
+                        double T2;
+                        if constexpr (TT == TT_STRAIGHT) {
+                            T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
+                        } else {
+                            double2 C = make_double2(0.0, 0.0);
+                            if constexpr (HAS_C) C = reinterpret_cast<const double2 *>(recA + 2 * RECS)[ri];
+                            T2 = exact_time_samples<TT>(P, ts, s, B, C);
+                        }
                         // s + 2^31 keeps s in the mantissa with 21 fraction bits
                         const double v = T2 + magic;
                         const unsigned vh = (unsigned)__double2hiint(v), vl = (unsigned)__double2loint(v);
@@ -700,7 +779,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         ok = act && iu < ns_m1;   // also rejects s < 0 and NaN
                         i0 = ok ? (int)iu : 0;
                         f = __uint_as_float(0x3F800000u | ((vl & 0x1FFFFFu) << 2)) - 1.0f;
-                        T = double_to_float_trunc(T2);   // T2 >= 2e-10: A >= 1e-20
+                        // straight: T2 >= 2e-10 (A >= 1e-20); the other kinds can give T2 = 0
+                        T = TT == TT_STRAIGHT ? double_to_float_trunc(T2) : (float)T2;
                     } else {
                         const float4 B = reinterpret_cast<const float4 *>(recA + RECS)[ri];
                         float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -764,14 +844,21 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     bool ok;
                     if constexpr (EXACT) {
                         const double2 B = reinterpret_cast<const double2 *>(recA + RECS)[ri];
-                        const double T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
+                        double T2;
+                        if constexpr (TT == TT_STRAIGHT) {
+                            T2 = sqrt_newton(fma(B.x, s.B, ts.A)) + sqrt_newton(fma(B.y, s.B, ts.A));
+                        } else {
+                            double2 C = make_double2(0.0, 0.0);
+                            if constexpr (HAS_C) C = reinterpret_cast<const double2 *>(recA + 2 * RECS)[ri];
+                            T2 = exact_time_samples<TT>(P, ts, s, B, C);
+                        }
                         const double v = T2 + magic;
                         const unsigned vh = (unsigned)__double2hiint(v), vl = (unsigned)__double2loint(v);
                         const unsigned iu = __funnelshift_r(vl, vh, 21);
                         ok = iu < ns_m1;
                         i0 = ok ? (int)iu : 0;
                         f = __uint_as_float(0x3F800000u | ((vl & 0x1FFFFFu) << 2));   // 1 + fraction
-                        T = double_to_float_trunc(T2);
+                        T = TT == TT_STRAIGHT ? double_to_float_trunc(T2) : (float)T2;
                     } else {
                         const float4 B = reinterpret_cast<const float4 *>(recA + RECS)[ri];
                         float4 Cc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -944,7 +1031,6 @@ __device__ __forceinline__ void init_barriers(CtaShared &sh) {
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
 __global__ void __launch_bounds__(kThreads, 1)
 migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
-    static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
     static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ CtaShared sh;
@@ -965,18 +1051,20 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
 
 // Persistent form for many outputs (offset bins): one CTA per SM fetches
 // items from a work counter; items of the bins with the most traces come
-// first (the host orders `bins`), so uneven bins balance.
+// first (the host orders `bins`), so uneven bins balance.  With a scatter
+// schedule (sw.boxes non-null) the items are (segment, pillar block, time
+// block) of P.image / P.fold, numbered segment by segment; an item finds its
+// segment by binary search in the segments' inclusive prefix counts.
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
 __global__ void __launch_bounds__(kThreads, 1)
 migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const BinWork *__restrict__ bins,
-                          int n_bins, unsigned long long *work_counter) {
-    static_assert(!EXACT || TT == TT_STRAIGHT, "the FP64 sample-index path is straight-ray only");
+                          int n_bins, unsigned long long *work_counter, const ScatterWork sw) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ CtaShared sh;
     init_barriers(sh);
     const int n_pblk_x = (P.nx + P.px - 1) / P.px;
     const long long per_bin = (long long)n_pblk_x * P.n_pblk_y * P.n_tblk;
-    const long long n_items = per_bin * n_bins;
+    const long long n_items = sw.boxes ? (sw.n_seg > 0 ? sw.ends[sw.n_seg - 1] : 0) : per_bin * n_bins;
     int64_t chunk_base = 0;
     for (;;) {
         __syncthreads();
@@ -984,6 +1072,36 @@ migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const
         __syncthreads();
         const long long item = sh.item;
         if (item >= n_items) break;
+        if (sw.boxes) {
+            __shared__ int64_t s_seg;
+            if (threadIdx.x == 0) {   // the first segment whose inclusive count exceeds the item
+                int64_t lo = 0, hi = sw.n_seg - 1;
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi) >> 1;
+                    if (sw.ends[mid] > item) hi = mid;
+                    else lo = mid + 1;
+                }
+                s_seg = lo;
+            }
+            __syncthreads();
+            const int64_t seg = s_seg;
+            const SegmentBox bx = sw.boxes[seg];
+            long long k = item - (seg > 0 ? sw.ends[seg - 1] : 0);
+            const int nby = bx.pby1 - bx.pby0 + 1;
+            Item it;
+            it.tblock = (int)(k % P.n_tblk);
+            k /= P.n_tblk;
+            it.pby = bx.pby0 + (int)(k % nby);
+            it.pbx = bx.pbx0 + (int)(k / nby);
+            it.trace0 = seg * sw.seg_traces;
+            it.n_traces = min(sw.seg_traces, P.n_traces - it.trace0);
+            it.amps = reinterpret_cast<const unsigned char *>(P.amps) + it.trace0 * P.amp_stride * P.elem;
+            it.geo = P.geo + it.trace0 * kGeoDoubles;
+            it.image = P.image;
+            it.fold = P.fold;
+            if (!migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base)) break;
+            continue;
+        }
         const BinWork &bw = bins[item / per_bin];
         long long rem = item - (item / per_bin) * per_bin;
         Item it;

@@ -35,7 +35,7 @@ static cudaError_t opt_in_smem(SmemOptIn &state, Kernel kern, size_t smem) {
 
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
 static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L) {
-    if (!L.bins) {
+    if (!L.bins && !L.scatter.boxes) {
         auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
         static SmemOptIn opt_in;   // per instantiation
         cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
@@ -62,7 +62,7 @@ static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L
         if (L.ctas_out) *L.ctas_out = ctas;
         return cudaSuccess;
     }
-    kern<<<ctas, kThreads, L.smem, L.stream>>>(P, Pg, L.bins, L.n_bins, L.counter);
+    kern<<<ctas, kThreads, L.smem, L.stream>>>(P, Pg, L.bins, L.n_bins, L.counter, L.scatter);
     return cudaGetLastError();
 }
 
@@ -83,12 +83,10 @@ static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, boo
     return cudaErrorInvalidValue;
 }
 
-// exact: FP64 sample index (straight rays only); otherwise FP32 traveltime.
+// exact: FP64 sample index; otherwise FP32 traveltime.
 template <int TT>
 cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact, const Launch &L) {
-    if constexpr (TT == TT_STRAIGHT) {
-        if (exact) return launch_prec<TT, true>(P, Pg, amp, vel3d, L);
-    }
+    if (exact) return launch_prec<TT, true>(P, Pg, amp, vel3d, L);
     return launch_prec<TT, false>(P, Pg, amp, vel3d, L);
 }
 

@@ -51,9 +51,11 @@ constexpr size_t kOffTimeA = kOffTime + size_t(kMaxTimes) * 32;   // double per 
 constexpr size_t kOffTab = kOffTimeA + size_t(kMaxTimes) * 8;     // float4 per entry
 constexpr size_t kOffBtab = kOffTab + size_t(kMaxTable) * 16;     // double per entry
 constexpr size_t kOffGeo = kOffBtab + size_t(kMaxTable) * 8;      // 8 doubles per trace
+constexpr size_t kOffTimeV = kOffGeo + size_t(kMaxTraces) * kGeoDoubles * 8;   // double per time
 static_assert(sizeof(KParams) <= kOffErr && sizeof(KParams) % 4 == 0, "launch parameters overlap the error word");
-static_assert(kOffGeo + size_t(kMaxTraces) * kGeoDoubles * 8 <= kScratchBytes, "scratch layout overflows");
-static_assert(kOffTab % 256 == 0 && kOffGeo % 256 == 0, "scratch regions must stay 256-byte aligned");
+static_assert(kOffTimeV + size_t(kMaxTimes) * 8 <= kScratchBytes, "scratch layout overflows");
+static_assert(kOffTab % 256 == 0 && kOffGeo % 256 == 0 && kOffTimeV % 256 == 0,
+              "scratch regions must stay 256-byte aligned");
 
 // The scratch array.  Host code must not use the symbol as a pointer: it is a
 // host-side stand-in.  Its device address comes from cudaGetSymbolAddress.
@@ -136,11 +138,12 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     plan::choose_shape(out->nt, 0, 0, R, PB);
     KParams P = plan::make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // image += 0, fold += 0
-    const bool exact = prm->precision == PSTM_PREC_EXACT && prm->traveltime == PSTM_TT_STRAIGHT;
+    const bool exact = prm->precision == PSTM_PREC_EXACT;
     P.exact_units = exact ? 1 : 0;
     P.curved_kind = (prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) ? 1 : 0;
     P.ttime = reinterpret_cast<const float4 *>(scratch + kOffTime);
     P.ttimeA = reinterpret_cast<const double *>(scratch + kOffTimeA);
+    P.ttimeV = reinterpret_cast<const double *>(scratch + kOffTimeV);
     P.ttab = reinterpret_cast<const float4 *>(scratch + kOffTab);
     P.btab = reinterpret_cast<const double *>(scratch + kOffBtab);
     P.geo = reinterpret_cast<const double *>(scratch + kOffGeo);
@@ -159,7 +162,8 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     prep_time_table<<<blocks, 256, 0, st>>>(P, n_p, reinterpret_cast<float4 *>(scratch + kOffTab),
                                             reinterpret_cast<double *>(scratch + kOffBtab),
                                             reinterpret_cast<float4 *>(scratch + kOffTime),
-                                            reinterpret_cast<double *>(scratch + kOffTimeA));
+                                            reinterpret_cast<double *>(scratch + kOffTimeA),
+                                            reinterpret_cast<double *>(scratch + kOffTimeV));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "prep_time_table launch");
     blocks = (int)((tr->n_traces + 255) / 256);
     if (blocks > 148 * 32) blocks = 148 * 32;

@@ -132,6 +132,9 @@ inline KParams make_params(const pstm_traces_desc *tr, const pstm_output_desc *o
                        ((prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) &&
                         !P.cr_k_zero)) ? 1 : 0;
     P.compensated = prm->compensated ? 1 : 0;
+    P.cr_B0 = 1.0 / (prm->curved_v0 * prm->curved_v0 * P.dt_s * P.dt_s);
+    P.cr_k2 = prm->curved_k * prm->curved_k;
+    P.cr_inv_k_dt = P.cr_k_zero ? 0.0 : 1.0 / (prm->curved_k * P.dt_s);
     P.wait_iters = kWaitIters;
     // Fault injection for the tests of the bounded waits: PSTM_CUDA_INJECT_FAULT=wait
     // leaves the first trace chunks' copies unissued, so the kernel's bounded

@@ -5,11 +5,12 @@
 namespace pstm {
 
 // Per-(pillar or 0, output time): {1/v^2, aperture, 1/v, eta} and 1/(v dt)^2;
-// per output time: {t0h2, Kt, tg, tguard}, {vz, vz2, 1/vz, t0 == 0} and
-// (t0/(2 dt))^2.  Evaluated in FP64 as numba_cpu_optimized.py:378-399 does;
-// the float4s are rounded once to FP32.
+// per output time: {t0h2, Kt, tg, tguard}, {vz, vz2, 1/vz, t0 == 0},
+// (t0/(2 dt))^2 and (curved kinds, when ttimeV is given) v(z) in FP64.
+// Evaluated in FP64 as numba_cpu_optimized.py:378-399 does; the float4s are
+// rounded once to FP32.
 __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, double *btab, float4 *ttime,
-                                double *ttimeA) {
+                                double *ttimeA, double *ttimeV) {
     const int64_t n = n_p * P.nt;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -38,6 +39,7 @@ __global__ void prep_time_table(const KParams P, int64_t n_p, float4 *tab, doubl
                 vz = (float)vzd;
                 vz2 = (float)(vzd * vzd);
                 ivwc = (float)(1.0 / vzd);
+                if (ttimeV) ttimeV[t] = vzd;
             }
             ttime[2 * t] = make_float4((float)((t0 * 0.5) * (t0 * 0.5)), P.obliquity ? (float)(t0 / tu) : 1.f,
                                        small_t ? (float)tguard : -1.f, (float)tguard);

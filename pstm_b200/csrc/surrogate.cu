@@ -400,7 +400,12 @@ __global__ void __launch_bounds__(128) migrate_learned_kernel(const KParams P, c
     const int tc = tv ? t : P.nt - 1;
     TimeState ts;
     PtState s;
-    load_states<TT_STRAIGHT, false>(P, p, t, ts, s);   // s.ap < 0 past the tile end
+    // the weight tables are in samples when the tile was prepared for the FP64
+    // sample-index kernel (its exact fallback), else in seconds; T is in seconds
+    const bool samples = P.exact_units != 0;
+    if (samples) load_states<TT_STRAIGHT, true>(P, p, t, ts, s);   // s.ap < 0 past the tile end
+    else load_states<TT_STRAIGHT, false>(P, p, t, ts, s);
+    const float tw = samples ? P.inv_dt_f : 1.f;   // T in the weights' unit
     const float4 tab = P.ttab[(P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc];
     const float t0 = (float)(P.ta[tc] / 1000.0), v = 1.f / tab.z, eta = tab.w;
     const bool w_one = P.spreading + P.obliquity == 1, w_two = P.spreading + P.obliquity == 2;
@@ -437,13 +442,14 @@ __global__ void __launch_bounds__(128) migrate_learned_kernel(const KParams P, c
             float wt = ok ? (float)g[6] : 0.f;
             const float x = fmaf(d, s.itw, s.tsn);
             wt *= x > 0.f ? taper_weight(x) : 1.f;
-            const float rT = rcp_approx(T);
+            const float Tw = T * tw;
+            const float rT = rcp_approx(Tw);
             float gw = w_two ? s.K * rT * rT : (w_one ? s.K * rT : 1.f);
-            gw = T > ts.tg ? gw : 1.f;
+            gw = Tw > ts.tg ? gw : 1.f;
             if (P.aa) {
                 const float sth = fminf((float)fmax(fabs(dxm), fabs(dym)) * s.ivw_t * rT, 1.f);
                 const float aa = fmaxf(0.f, 1.f - fmaxf(s.aaA * sth, P.aa_cB));
-                gw = (sth >= 0.01f && T >= ts.tguard) ? gw * aa : gw;
+                gw = (sth >= 0.01f && Tw >= ts.tguard) ? gw * aa : gw;
             }
             acc = fmaf(amp, wt * gw, acc);
         }

@@ -497,7 +497,24 @@ class CudaKernel:
         r = np.ascontiguousarray(np.asarray(runs, dtype=np.int64).reshape(-1, 2))
         return self._migrate(traces, output, velocity, config, _TT_BY_TYPE[kernel_type], runs=r)
 
-    def _migrate(self, traces, output, velocity, config, tt: int, runs=None) -> KernelMetrics:
+    def migrate_scatter(self, traces, output, velocity, config=None, kernel_type: str = "straight_ray",
+                        segment_traces: int = 0, count_items: bool = False) -> KernelMetrics:
+        """Migrate an output grid with the trace-centric (scatter) schedule:
+        every trace is read once for the whole grid, as in the reference's
+        trace-centric kernel (``pstm_trace_centric.metal:112-236``), with the
+        gather kernel's partial sums and one atomic add per output sample per
+        (segment, pillar block, time block) item.  ``traces`` are CUDA tensors,
+        best in midpoint order (``pstm_b200.spatial.sort_panel``); the output
+        has a regular grid (ascending ``x_axis``, ``y_axis``).  The result is
+        ``migrate_tile``'s up to the order of floating-point additions.  With
+        ``count_items`` the call synchronises and the metrics carry the number
+        of items in ``n_items``."""
+        if kernel_type not in _TT_BY_TYPE:
+            raise ValueError(f"unknown kernel_type {kernel_type!r}")
+        return self._migrate(traces, output, velocity, config, _TT_BY_TYPE[kernel_type],
+                             scatter=(int(segment_traces), bool(count_items)))
+
+    def _migrate(self, traces, output, velocity, config, tt: int, runs=None, scatter=None) -> KernelMetrics:
         if self._ctx is None or self._config is None:
             raise RuntimeError("Kernel not initialized")
         cfg = config if config is not None else self._config
@@ -560,6 +577,21 @@ class CudaKernel:
             nat.check(rc, self._ctx, self._lib)
             return KernelMetrics(n_traces_processed=int((runs[:, 1] - runs[:, 0]).sum()) if len(runs) else 0,
                                  n_samples_output=nx * ny * nt, compute_time_s=time.perf_counter() - t_start)
+        if scatter is not None:
+            if not on_dev:
+                raise ValueError("migrate_scatter takes CUDA tensors only")
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
+            n_items = ctypes.c_int64(0)
+            rc = self._lib.pstm_cuda_migrate_scatter_dev(
+                self._ctx, ctypes.byref(td), scatter[0], ctypes.byref(od), ctypes.byref(vd), ctypes.byref(prm),
+                ctypes.byref(n_items) if scatter[1] else None, ctypes.c_void_p(stream))
+            nat.check(rc, self._ctx, self._lib)
+            m = KernelMetrics(n_traces_processed=ntr, n_samples_output=nx * ny * nt,
+                              compute_time_s=time.perf_counter() - t_start)
+            if scatter[1]:
+                m.n_items = int(n_items.value)
+            return m
         if on_dev:
             import torch   # order the launch after the producers of the caller's tensors
             stream = torch.cuda.current_stream().cuda_stream or nat.STREAM_LEGACY
