@@ -62,7 +62,10 @@ class TiledExecutor:
     full grid's axes (NumPy).  ``spatial`` (True, or a column width in m;
     True takes an eighth of a tile's width) sorts the panel into midpoint order
     once -- a second copy of the panel while the caller holds the first -- and
-    migrates each tile against its row ranges in place.
+    migrates each tile against its row ranges in place.  Without it, a
+    midpoint index on the host selects each tile's traces (no per-tile scan of
+    the panel) and they are gathered into a tile panel.  Panels larger than
+    HBM: ``pstm_b200.streaming.StreamingExecutor``.
     """
 
     def __init__(self, kernel, traces, x_axis, y_axis, t_axis_ms, velocity, config,
@@ -82,17 +85,23 @@ class TiledExecutor:
         self.max_residual_ms = max_residual_ms
         dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
         self._x, self._y, self._t = dev(self.x_axis), dev(self.y_axis), dev(self.t_axis_ms)
+        from .spatial import MidpointIndex, sort_panel
+        if spatial is True or spatial is False or spatial is None:
+            dx = abs(float(self.x_axis[1] - self.x_axis[0])) if len(self.x_axis) > 1 else 1.0
+            width = max(self.tile * dx / 8.0, 1e-3)
+        else:
+            width = float(spatial)
+        host = lambda a: a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+        # The midpoint index finds a tile's traces in O(log n + selected) on the
+        # host instead of a mask over the whole panel per tile.  Only the
+        # spatial mode reorders the panel itself (one copy of it).
+        midx = MidpointIndex(host(traces.midpoint_x), host(traces.midpoint_y), width)
         self.index = None
         if spatial is not False and spatial is not None:
-            from .spatial import MidpointIndex, sort_panel
-            if spatial is True:
-                dx = abs(float(self.x_axis[1] - self.x_axis[0])) if len(self.x_axis) > 1 else 1.0
-                width = max(self.tile * dx / 8.0, 1e-3)
-            else:
-                width = float(spatial)
-            host = lambda a: a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
-            self.index = MidpointIndex(host(traces.midpoint_x), host(traces.midpoint_y), width)
+            self.index = midx
             self.tb = sort_panel(traces, self.index)
+        else:
+            self._lookup = midx
 
     def tiles(self):
         return tile_ranges(len(self.x_axis), len(self.y_axis), self.tile)
@@ -100,11 +109,10 @@ class TiledExecutor:
     def select(self, tile):
         """Indices (CUDA int64, ascending) of the traces that can reach the tile."""
         x_lo, x_hi, y_lo, y_hi = selection_box(self.x_axis, self.y_axis, tile, self.cfg.max_aperture_m)
-        if self.index is not None:
+        if self.index is not None:   # positions in the sorted panel
             return self.torch.as_tensor(self.index.select(x_lo, x_hi, y_lo, y_hi), device="cuda")
-        mx, my = self.tb.midpoint_x, self.tb.midpoint_y
-        m = (mx >= x_lo) & (mx <= x_hi) & (my >= y_lo) & (my <= y_hi)
-        return self.torch.nonzero(m).squeeze(1)
+        pos = self._lookup.select(x_lo, x_hi, y_lo, y_hi)   # positions in midpoint order
+        return self.torch.as_tensor(np.sort(self._lookup.order[pos]), device="cuda")
 
     def _gather(self, idx):
         from .base import TraceBlock
