@@ -61,6 +61,10 @@ constexpr int kWaitIters = 1 << 20;  // default bound of every mbarrier wait loo
 #ifndef PSTM_PACKED_PAIRS
 #define PSTM_PACKED_PAIRS 1
 #endif
+// Unroll factor of the packed loop (steps of two records).
+#ifndef PSTM_UNROLL_PACKED
+#define PSTM_UNROLL_PACKED 2
+#endif
 #define PSTM_PRAGMA_STR(x) #x
 #define PSTM_UNROLL(n) _Pragma(PSTM_PRAGMA_STR(unroll n))
 
@@ -916,7 +920,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     } else if (PSTM_PACKED_PAIRS) {
                         float2 acc = make_float2(0.f, 0.f);
                         int c = 0;
-                        PSTM_UNROLL(2)
+                        PSTM_UNROLL(PSTM_UNROLL_PACKED)
                         for (; c + 1 < n0; c += 2) plain2(c, acc);
                         if (c < n0) a += pair(c, F{}, F{}, F{}, F{}, Tr{});
                         a += acc.x + acc.y;
