@@ -464,9 +464,10 @@ def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, 
     return res
 
 
-def measure_case1_interp(method: str = "sinc8"):
-    """The case-1 tile with a higher-order trace interpolator (the FP64
-    interpolation kernel) instead of linear: pairs/s on device inputs."""
+def measure_case1_interp(method: str = "sinc8", precision: str = "exact"):
+    """The case-1 tile with a higher-order trace interpolator instead of
+    linear: pairs/s on device inputs.  precision "exact" runs the FP64
+    interpolation kernel, "fast" its FP64-index / FP32-tap variant."""
     import dataclasses
     import torch
     from pstm_b200 import workloads
@@ -484,7 +485,7 @@ def measure_case1_interp(method: str = "sinc8"):
                    fold=torch.zeros(out.fold.shape, dtype=torch.int32, device="cuda"),
                    x_axis=dev(out.x_axis), y_axis=dev(out.y_axis), t_axis_ms=dev(out.t_axis_ms))
     vel = VelocitySlice(vrms=dev(case.velocity.vrms), is_1d=True)
-    k = CudaKernel()
+    k = CudaKernel(precision=precision)
     k.initialize(cfg)
     k.migrate_tile(dtb, o, vel, cfg)
     torch.cuda.synchronize()
@@ -496,7 +497,9 @@ def measure_case1_interp(method: str = "sinc8"):
     k.cleanup()
     ms = e0.elapsed_time(e1)
     return {"value": case.pairs / (ms / 1e3), "unit": UNIT, "ms_per_tile": ms, "interpolation": method,
-            "workload": "case 1 tile with the FP64 higher-order interpolation kernel"}
+            "precision": precision,
+            "workload": "case 1 tile with the higher-order interpolation kernel "
+                        + ("(FP64 throughout)" if precision == "exact" else "(FP64 index, FP32 taps and weights)")}
 
 
 def measure_case1():
@@ -966,6 +969,7 @@ def main_ours(args):
         forms = measure_forms(args, k, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg)
         forms["case1_tile"] = measure_case1()
         forms["case1_tile_sinc8"] = measure_case1_interp("sinc8")
+        forms["case1_tile_sinc8_fast"] = measure_case1_interp("sinc8", "fast")
     if not args.no_batched and single:
         forms = forms or {}
         forms["batched_offset_bins_bf16_vti"] = measure_batched(args, world, dist, scale=args.batch_scale,

@@ -6,8 +6,10 @@
 // Catmull-Rom cubic, Hanning-windowed sinc of 4/8/16 points and Lanczos 3/5,
 // the wide ones falling back to linear within their half-width of a trace end
 // and normalising by the sum of their weights.  Linear interpolation stays on
-// the tiled gather kernel; the other methods run here, in FP64 (traveltime,
-// sample index, interpolation weights and accumulation), with one CTA of 128
+// the tiled gather kernel; the other methods run here -- in FP64 (traveltime,
+// sample index, interpolation weights and accumulation) on the exact path, with
+// FP32 taps, interpolation and weights after the FP64 sample index on the fast
+// path -- with one CTA of 128
 // threads per (pillar, block of 128 output times) and the traces read from
 // the packed geometry and the caller's panel.  Each warp stages the traces 32
 // at a time in a shared-memory slice of its own: each lane takes one trace's
@@ -40,33 +42,39 @@ constexpr int kInterpThreads = 128;
 #define PSTM_INTERP_MIN_CTAS 8
 #endif
 
-template <int AMP>
-__device__ inline double sample_at(const unsigned char *row, int64_t i) {
-    return (double)amp_at<AMP>(row, (int)i);
+template <int AMP, typename R = double>
+__device__ inline R sample_at(const unsigned char *row, int64_t i) {
+    return (R)amp_at<AMP>(row, (int)i);
 }
+
+// sincospi in the interpolation arithmetic: FP64, or FP32 on the fast path.
+__device__ inline void sincospi_r(double x, double *s, double *c) { sincospi(x, s, c); }
+__device__ inline void sincospi_r(float x, float *s, float *c) { sincospif(x, s, c); }
 
 // Nearest, Catmull-Rom cubic and linear interpolation at fractional index t
 // (0 <= t < ns - 1 is checked by the caller); linear also serves the wide
 // methods within their half-width of a trace end.
-template <int AMP>
-__device__ double interpolate_narrow(const unsigned char *row, int ns, double t, int method) {
+// R is the arithmetic of the weights and taps: double (exact path) or float
+// (fast path); the sample index t is FP64 in both.
+template <int AMP, typename R>
+__device__ R interpolate_narrow(const unsigned char *row, int ns, double t, int method) {
     if (method == PSTM_INTERP_NEAREST) {
         const int64_t i = (int64_t)(t + 0.5);
-        return (i < 0 || i >= ns) ? 0.0 : sample_at<AMP>(row, i);
+        return (i < 0 || i >= ns) ? R(0) : sample_at<AMP, R>(row, i);
     }
     if (method == PSTM_INTERP_CUBIC && t >= 1.0 && t < (double)(ns - 2)) {   // Catmull-Rom
         const int64_t i = (int64_t)t;
-        const double u = t - (double)i;
-        const double p0 = sample_at<AMP>(row, i - 1), p1 = sample_at<AMP>(row, i);
-        const double p2 = sample_at<AMP>(row, i + 1), p3 = sample_at<AMP>(row, i + 2);
-        const double c3 = -0.5 * p0 + 1.5 * p1 - 1.5 * p2 + 0.5 * p3;
-        const double c2 = p0 - 2.5 * p1 + 2.0 * p2 - 0.5 * p3;
-        const double c1 = -0.5 * p0 + 0.5 * p2;
+        const R u = (R)(t - (double)i);
+        const R p0 = sample_at<AMP, R>(row, i - 1), p1 = sample_at<AMP, R>(row, i);
+        const R p2 = sample_at<AMP, R>(row, i + 1), p3 = sample_at<AMP, R>(row, i + 2);
+        const R c3 = R(-0.5) * p0 + R(1.5) * p1 - R(1.5) * p2 + R(0.5) * p3;
+        const R c2 = p0 - R(2.5) * p1 + R(2.0) * p2 - R(0.5) * p3;
+        const R c1 = R(-0.5) * p0 + R(0.5) * p2;
         return ((c3 * u + c2) * u + c1) * u + p1;
     }
     const int64_t i0 = (int64_t)t;
-    const double f = t - (double)i0;
-    return sample_at<AMP>(row, i0) * (1.0 - f) + sample_at<AMP>(row, i0 + 1) * f;
+    const R f = (R)(t - (double)i0);
+    return sample_at<AMP, R>(row, i0) * (R(1) - f) + sample_at<AMP, R>(row, i0 + 1) * f;
 }
 
 // Windowed sinc (LANCZOS false) or Lanczos (true) of half-width HW at
@@ -86,36 +94,37 @@ __device__ double interpolate_narrow(const unsigned char *row, int ns, double t,
 // otherwise those of the direct formulas: sinc(x) = sin(pi x) / (pi x) with 1
 // for |x| < 1e-10, a Hann window 0.5 (1 + cos(pi x / HW)) that is 0 for
 // |x| >= HW, Lanczos sinc(x) sinc(x / HW).
-template <int AMP, int HW, bool LANCZOS>
-__device__ double interpolate_wide(const unsigned char *row, int ns, double t, double cos_d, double sin_d) {
+template <int AMP, int HW, bool LANCZOS, typename R>
+__device__ R interpolate_wide(const unsigned char *row, int ns, double t, R cos_d, R sin_d) {
     if (t < (double)HW || t >= (double)(ns - HW)) {
         const int64_t i0 = (int64_t)t;
-        const double f = t - (double)i0;
-        return sample_at<AMP>(row, i0) * (1.0 - f) + sample_at<AMP>(row, i0 + 1) * f;
+        const R f = (R)(t - (double)i0);
+        return sample_at<AMP, R>(row, i0) * (R(1) - f) + sample_at<AMP, R>(row, i0 + 1) * f;
     }
     const int64_t ic = LANCZOS ? (int64_t)t : (int64_t)(t + 0.5);
-    const double frac = t - (double)ic;
-    double s_f, c_f;
-    sincospi(frac, &s_f, &c_f);
-    double acc = 0.0, norm = 0.0;
-    auto tap = [&](int k, double s_k, double s_w, double c_w) {
+    const R frac = (R)(t - (double)ic);
+    const R pi = (R)M_PI;
+    R s_f, c_f;
+    sincospi_r(frac, &s_f, &c_f);
+    R acc = R(0), norm = R(0);
+    auto tap = [&](int k, R s_k, R s_w, R c_w) {
         const int64_t i = ic + k;
         if (i < 0 || i >= ns) return;   // (sinc rounds to the nearest sample: ic + HW can reach ns)
-        const double x = frac - (double)k;
-        double w;
-        if (LANCZOS) w = fabs(x) < 1e-10 ? 1.0 : (fabs(x) >= HW ? 0.0 : (s_k * s_w * HW) / (M_PI * M_PI * x * x));
-        else w = (fabs(x) < 1e-10 ? 1.0 : s_k / (M_PI * x)) * (fabs(x) >= HW ? 0.0 : 0.5 * (1.0 + c_w));
-        acc += sample_at<AMP>(row, i) * w;
+        const R x = frac - (R)k;
+        R w;
+        if (LANCZOS) w = fabs(x) < R(1e-10) ? R(1) : (fabs(x) >= R(HW) ? R(0) : (s_k * s_w * R(HW)) / (pi * pi * x * x));
+        else w = (fabs(x) < R(1e-10) ? R(1) : s_k / (pi * x)) * (fabs(x) >= R(HW) ? R(0) : R(0.5) * (R(1) + c_w));
+        acc += sample_at<AMP, R>(row, i) * w;
         norm += w;
     };
     if (!LANCZOS) {   // one chain, k = -HW+1 .. HW, window angle dropping by pi / HW per tap
-        double s_w, c_w;
-        sincospi((frac + (double)(HW - 1)) / (double)HW, &s_w, &c_w);
-        double s_k = ((HW - 1) & 1) ? -s_f : s_f;
+        R s_w, c_w;
+        sincospi_r((frac + (R)(HW - 1)) / (R)HW, &s_w, &c_w);
+        R s_k = ((HW - 1) & 1) ? -s_f : s_f;
 #pragma unroll
         for (int k = -HW + 1; k <= HW; ++k) {
             tap(k, s_k, s_w, c_w);
-            const double c_n = c_w * cos_d + s_w * sin_d;
+            const R c_n = c_w * cos_d + s_w * sin_d;
             s_w = s_w * cos_d - c_w * sin_d;
             c_w = c_n;
             s_k = -s_k;
@@ -123,21 +132,21 @@ __device__ double interpolate_wide(const unsigned char *row, int ns, double t, d
     } else {          // k = 0, -1, .., -HW+1 (angle growing), then k = 1, .., HW (angle dropping)
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
-            const double sin_a = side ? -sin_d : sin_d;
-            double s_w, c_w;
-            sincospi((frac - (double)side) / (double)HW, &s_w, &c_w);
-            double s_k = side ? -s_f : s_f;
+            const R sin_a = side ? -sin_d : sin_d;
+            R s_w, c_w;
+            sincospi_r((frac - (R)side) / (R)HW, &s_w, &c_w);
+            R s_k = side ? -s_f : s_f;
 #pragma unroll
             for (int n = 0; n < HW; ++n) {
                 tap(side ? 1 + n : -n, s_k, s_w, c_w);
-                const double c_n = c_w * cos_d - s_w * sin_a;
+                const R c_n = c_w * cos_d - s_w * sin_a;
                 s_w = s_w * cos_d + c_w * sin_a;
                 c_w = c_n;
                 s_k = -s_k;
             }
         }
     }
-    return norm > 1e-10 ? acc / norm : 0.0;
+    return norm > R(1e-10) ? acc / norm : R(0);
 }
 
 template <int TT>
@@ -151,7 +160,10 @@ struct Staged {
     int tr[32];
 };
 
-template <int AMP, int HW, bool LANCZOS>
+// R: double on the exact path (FP64 end to end); float on the fast path,
+// where only the traveltime, the sample index and the accumulation stay FP64
+// and the taps, the interpolation and the weights are FP32.
+template <int AMP, int HW, bool LANCZOS, typename R>
 __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_interp_kernel(const KParams P, int tt, int method) {
     __shared__ Staged S_all[kInterpThreads / 32];
     const int p = blockIdx.x;
@@ -175,8 +187,8 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
     const double gmax = P.aa_gmax, fdom = P.aa_fdom;
     const double inv_vw = 1.0 / vw;
     const double taper_start = ap * (1.0 - P.taper);
-    double sin_d = 0.0, cos_d = 1.0;
-    if (HW > 0) sincospi(1.0 / (double)HW, &sin_d, &cos_d);
+    R sin_d = R(0), cos_d = R(1);
+    if (HW > 0) sincospi_r(R(1) / (R)HW, &sin_d, &cos_d);
 
     Staged &S = S_all[warp];
     // Largest aperture over the warp's output times: a trace farther than it
@@ -229,23 +241,30 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             if (!(s >= 0.0 && s < (double)(P.ns - 1))) continue;
             const unsigned char *row =
                 reinterpret_cast<const unsigned char *>(P.amps) + ((int64_t)S.tr[j] * P.amp_stride) * (int64_t)P.elem;
-            double amp;
-            if (HW > 0) amp = interpolate_wide<AMP, HW, LANCZOS>(row, P.ns, s, cos_d, sin_d);
-            else amp = interpolate_narrow<AMP>(row, P.ns, s, method);
-            double w = S.w[j];
-            if (dj > taper_start) w *= 0.5 * (1.0 + cospi((dj - taper_start) / (ap - taper_start)));
+            R amp;
+            if (HW > 0) amp = interpolate_wide<AMP, HW, LANCZOS, R>(row, P.ns, s, cos_d, sin_d);
+            else amp = interpolate_narrow<AMP, R>(row, P.ns, s, method);
+            R w = (R)S.w[j];
+            if (dj > taper_start) {
+                const R x = (R)((dj - taper_start) / (ap - taper_start));
+                R cw;
+                if constexpr (sizeof(R) == 8) cw = cospi(x);
+                else cw = cospif(x);
+                w *= R(0.5) * (R(1) + cw);
+            }
             // One reciprocal of T per pair and 1/v per thread serve the AA,
             // spreading and obliquity terms: sin = m / (v T), f_max = min(v /
             // (4 gmax sin), 500 Hz) so f_dom / f_max = f_dom max(4 gmax sin / v,
             // 1 / 500), spreading 1 / (v T), obliquity t0 / T.
-            const double inv_T = 1.0 / T;
+            const R Tr = (R)T, inv_T = R(1) / Tr, ivw = (R)inv_vw;
             if (P.aa && T >= 0.001) {
-                const double st = fmin(S.m[j] * inv_T * inv_vw, 1.0);
-                if (st >= 0.01) w *= fmax(0.0, 1.0 - fdom * fmax(4.0 * gmax * st * inv_vw, 1.0 / 500.0));
+                const R st = fmin((R)S.m[j] * inv_T * ivw, R(1));
+                if (st >= R(0.01))
+                    w *= fmax(R(0), R(1) - (R)fdom * fmax(R(4) * (R)gmax * st * ivw, R(1) / R(500)));
             }
-            if (P.spreading && T > 0.001) w *= inv_T * inv_vw;
-            if (P.obliquity && T > 0.001) w *= t0 * inv_T;
-            acc += amp * w;
+            if (P.spreading && T > 0.001) w *= inv_T * ivw;
+            if (P.obliquity && T > 0.001) w *= (R)t0 * inv_T;
+            acc += (double)(amp * w);
         }
         __syncwarp();   // the next batch overwrites the staged values
     }
@@ -260,7 +279,10 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
 
 template <int AMP, int HW, bool LANCZOS>
 void launch_one(const TilePlan &tp, dim3 grid, int method) {
-    migrate_interp_kernel<AMP, HW, LANCZOS><<<grid, kInterpThreads, 0, tp.L.stream>>>(tp.P, tp.tt, method);
+    if (tp.exact)
+        migrate_interp_kernel<AMP, HW, LANCZOS, double><<<grid, kInterpThreads, 0, tp.L.stream>>>(tp.P, tp.tt, method);
+    else
+        migrate_interp_kernel<AMP, HW, LANCZOS, float><<<grid, kInterpThreads, 0, tp.L.stream>>>(tp.P, tp.tt, method);
 }
 
 template <int AMP>

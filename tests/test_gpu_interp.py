@@ -1,7 +1,9 @@
 """Higher-order trace interpolation (nearest, cubic, windowed sinc, Lanczos)
 on the GPU against the FP64 oracle, whose interpolators are pinned to the
-reference's interpolate_sample.  The kernel works in FP64 like the oracle:
-relative L2 <= 1e-9, fold bit-exact."""
+reference's interpolate_sample.  On the exact path the kernel works in FP64
+like the oracle: relative L2 <= 1e-9, fold bit-exact.  On the fast path (FP64
+sample index, FP32 taps, interpolation and weights) the plain bar holds:
+relative L2 <= 1e-5."""
 from __future__ import annotations
 
 import numpy as np
@@ -13,14 +15,15 @@ from oracle import oracle
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("precision", ["exact", "fast"])
 @pytest.mark.parametrize("method", ["nearest", "cubic", "sinc4", "sinc8", "sinc16", "lanczos3", "lanczos5"])
-def test_interpolators_vs_oracle(method, cuda_kernel_factory):
+def test_interpolators_vs_oracle(method, precision, cuda_kernel_factory):
     import dataclasses
     from pstm_b200 import workloads
     from pstm_b200.base import OutputTile
     case = workloads.config1(n_traces=700, nx=6, ny=5, nt=500)
     cfg = dataclasses.replace(case.config, interpolation_method=method, aa_enabled=True)
-    k = cuda_kernel_factory(cfg)
+    k = cuda_kernel_factory(cfg, precision=precision)
     out = case.output
     k.migrate_tile(case.traces, out, case.velocity, cfg)
     ref = OutputTile(image=np.zeros(out.image.shape), fold=np.zeros(out.fold.shape, np.int32), x_axis=out.x_axis,
@@ -28,7 +31,7 @@ def test_interpolators_vs_oracle(method, cuda_kernel_factory):
     oracle.migrate(case.traces, ref, case.velocity, cfg)
     np.testing.assert_array_equal(out.fold, ref.fold)
     assert np.abs(ref.image).max() > 0
-    assert rel_l2(out.image, ref.image) <= 1e-9
+    assert rel_l2(out.image, ref.image) <= (1e-9 if precision == "exact" else 1e-5)
 
 
 def test_vti_sinc_and_device_path(cuda_kernel_factory):
