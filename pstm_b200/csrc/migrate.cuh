@@ -554,11 +554,11 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     // pillar q's 32 records, counts its fold and sorts them by midpoint
     // distance (bitonic, in registers) so that, for any aperture, the records
     // inside it form a prefix.
-    auto build_records = [&](int64_t k, int b) {
+    auto pillar_records = [&](int64_t k, int b, int q) {   // one warp: pillar q's records of chunk k
         const int64_t c0 = k * C;
         const int cmax = (int)min((int64_t)C, it.n_traces - c0);
-        if (warp < PB) {
-            const int q = warp, c = lane;
+        {
+            const int c = lane;
             const double *geo = reinterpret_cast<const double *>(geo_base + b * geo_buffer_bytes());
             float4 *recA = reinterpret_cast<float4 *>(rec_base + b * REC_BYTES);
             const int p = s_pid[q];
@@ -633,7 +633,12 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             else reinterpret_cast<float4 *>(recA + RECS)[ri] = Bf;
             if constexpr (HAS_C) reinterpret_cast<float4 *>(recA + 2 * RECS)[ri] = Cc;
         }
-        if (!P.bulk) {   // amplitude rows not 16-byte aligned: plain cooperative copy
+    };
+    // amplitude rows not 16-byte aligned (no TMA bulk copy): plain cooperative copy by all threads
+    auto copy_rows = [&](int64_t k, int b) {
+        const int64_t c0 = k * C;
+        const int cmax = (int)min((int64_t)C, it.n_traces - c0);
+        {
             unsigned char *dst = amp_base + b * amp_bytes;
             const unsigned char *src = it.amps;
             for (int e = tid; e < cmax * P.ns; e += kThreads) {
@@ -646,6 +651,10 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         reinterpret_cast<const unsigned short *>(src)[gi];
             }
         }
+    };
+    auto build_records = [&](int64_t k, int b) {   // every pillar (warp q < PB) and the row copy
+        if (warp < PB) pillar_records(k, b, warp);
+        if (!P.bulk) copy_rows(k, b);
     };
 
     // add this lane's FP32 partial sums into the FP64 (or FP32) image and clear them
@@ -713,13 +722,30 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         // shallow ones few, so a fixed warp-to-time mapping leaves the warps
         // with the shallow blocks idle at the chunk barrier.  A unit's partial
         // sums stay where the fixed mapping keeps them (lane vt of the block).
+        // The records of chunk k+1 (one task per pillar) are units of the same
+        // pool, numbered after the deepest time blocks: by then the chunk's copy
+        // has landed, and no warp is left to build them alone at the end.
         if (tid == 0) sh.unit[(k + 1) & 1] = 0;   // the next chunk's counter: chunk k-1 is done with it
+        const bool has_next = k + 1 < n_chunks;
+        const int nbuf = buf ^ 1;
+        const uint32_t nbar = nbuf ? bar1 : bar0, npar = (uint32_t)(((g + 1) >> 1) & 1);
+        const int n_rec = has_next ? PB : 0;
+        bool timeout = false;
 #pragma unroll 1
         for (;;) {
             int u = 0;
             if (lane == 0) u = atomicAdd(&sh.unit[k & 1], 1);
             u = __shfl_sync(0xffffffffu, u, 0);
-            if (u >= n_units) break;
+            if (u >= n_units + n_rec) break;
+            if (u >= units_per_r && u < units_per_r + n_rec) {   // records of chunk k+1, pillar u - units_per_r
+                if (!__all_sync(0xffffffffu, mbar_wait(nbar, npar, wait_iters))) {
+                    timeout = true;
+                    continue;
+                }
+                pillar_records(k + 1, nbuf, u - units_per_r);
+                continue;
+            }
+            if (u >= units_per_r) u -= n_rec;
             const int ur = u / units_per_r;           // 0 = the deepest r
             const int uw = u - ur * units_per_r;
             const int r = R - 1 - ur;
@@ -958,16 +984,19 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             }
         }
 
-        // ---------------- records of chunk k+1 (its copy was issued a chunk ago)
-        bool timeout = false;
-        if (k + 1 < n_chunks) {
-            const int nb = buf ^ 1;
-            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1), wait_iters);
-            if (!timeout) build_records(k + 1, nb);
-        }
         if (__syncthreads_or(timeout)) {   // also: buffer `buf` is free again
             aborted = true;
             break;
+        }
+        if (has_next) {
+            // every thread observes the completed phase of chunk k+1's copy (the
+            // record tasks saw it complete, so this returns at once); unaligned
+            // rows are then copied by all threads
+            mbar_wait(nbar, npar, wait_iters);
+            if (!P.bulk) {
+                copy_rows(k + 1, nbuf);
+                __syncthreads();
+            }
         }
         if ((k + 1) % flush_every == 0) {   // every unit of the chunk has added its sums
             flush();
