@@ -464,7 +464,6 @@ struct CtaShared {
     int rank[kMaxPB][kMaxChunk];
     unsigned long long bar[2];
     long long item;
-    int unit[2];   // work-unit counters of the pair loop, by chunk parity
 };
 
 // Migrates one item.  `chunk_base` counts the chunks this CTA staged before
@@ -496,7 +495,6 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     float *const s_err = s_acc + PB * R * kThreads;   // [PB][R][kThreads] when comp
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int kWarps = kThreads / 32;
     const int pbx = it.pbx, pby = it.pby;
     __syncthreads();   // the previous item is done with the shared state
     if (tid < PB) {
@@ -509,9 +507,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         s_oy[tid] = ok ? (P.yg ? P.yg[p] : P.ya[iy]) : 0.0;
     }
     const uint32_t bar0 = smem_u32(&sh.bar[0]), bar1 = smem_u32(&sh.bar[1]);
-    const int t_base = it.tblock * (kThreads * R);
-    const int t_lane = t_base + tid;   // this thread's times (flush, fold): t_lane + r * kThreads
-    const int units_per_r = PB * kWarps, n_units = units_per_r * R;
+    const int t_lane = it.tblock * (kThreads * R) + tid;   // this thread's times: t_lane + r * kThreads
 
     // hot-loop constants in registers
     const float s_scale = P.s_scale, s_offset = P.s_offset;
@@ -531,7 +527,6 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     const int flush_every = P.flush_every;
 
     for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
-    if (tid == 0) sh.unit[0] = sh.unit[1] = 0;
 
     // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
     // rows when they are 16-byte aligned) into buffer b
@@ -716,48 +711,16 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         const unsigned char *ampb = amp_base + buf * amp_bytes;
 
         // ---------------- pairs of chunk k
-        // Work units are (pillar, block of 32 output times); a warp takes the
-        // next unit from the CTA's counter for this chunk, deepest time blocks
-        // first.  Deep times have wide apertures and many records inside them,
-        // shallow ones few, so a fixed warp-to-time mapping leaves the warps
-        // with the shallow blocks idle at the chunk barrier.  A unit's partial
-        // sums stay where the fixed mapping keeps them (lane vt of the block).
-        // The records of chunk k+1 (one task per pillar) are units of the same
-        // pool, numbered after the deepest time blocks: by then the chunk's copy
-        // has landed, and no warp is left to build them alone at the end.
-        if (tid == 0) sh.unit[(k + 1) & 1] = 0;   // the next chunk's counter: chunk k-1 is done with it
-        const bool has_next = k + 1 < n_chunks;
-        const int nbuf = buf ^ 1;
-        const uint32_t nbar = nbuf ? bar1 : bar0, npar = (uint32_t)(((g + 1) >> 1) & 1);
-        const int n_rec = has_next ? PB : 0;
-        bool timeout = false;
 #pragma unroll 1
-        for (;;) {
-            int u = 0;
-            if (lane == 0) u = atomicAdd(&sh.unit[k & 1], 1);
-            u = __shfl_sync(0xffffffffu, u, 0);
-            if (u >= n_units + n_rec) break;
-            if (u >= units_per_r && u < units_per_r + n_rec) {   // records of chunk k+1, pillar u - units_per_r
-                if (!__all_sync(0xffffffffu, mbar_wait(nbar, npar, wait_iters))) {
-                    timeout = true;
-                    continue;
-                }
-                pillar_records(k + 1, nbuf, u - units_per_r);
-                continue;
-            }
-            if (u >= units_per_r) u -= n_rec;
-            const int ur = u / units_per_r;           // 0 = the deepest r
-            const int uw = u - ur * units_per_r;
-            const int r = R - 1 - ur;
-            const int wb = kWarps - 1 - uw / PB;      // time block within r, deepest first
-            const int q = uw - (kWarps - 1 - wb) * PB;
+        for (int q = 0; q < PB; ++q) {
             const int p = s_pid[q];
             if (p < 0) continue;
-            const int vt = wb * 32 + lane;            // the lane whose partial sums these are
             const float4 *A_q = recA + q * kMaxChunk;
             const float dl = A_q[lane].x;   // this lane's slot of the sorted distances
-            {
-                const int t = t_base + vt + r * kThreads;
+            const int vt = tid;             // the partial sums of this thread's times
+#pragma unroll 1
+            for (int r = 0; r < R; ++r) {
+                const int t = t_lane + r * kThreads;
                 TimeState ts;
                 PtState s;
                 load_states<TT, EXACT>(P, p, t, ts, s);
@@ -984,23 +947,17 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             }
         }
 
+        // ---------------- records of chunk k+1 (its copy was issued a chunk ago)
+        bool timeout = false;
+        if (k + 1 < n_chunks) {
+            const int nb = buf ^ 1;
+            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1), wait_iters);
+            if (!timeout) build_records(k + 1, nb);
+        }
+        if ((k + 1) % flush_every == 0) flush();
         if (__syncthreads_or(timeout)) {   // also: buffer `buf` is free again
             aborted = true;
             break;
-        }
-        if (has_next) {
-            // every thread observes the completed phase of chunk k+1's copy (the
-            // record tasks saw it complete, so this returns at once); unaligned
-            // rows are then copied by all threads
-            mbar_wait(nbar, npar, wait_iters);
-            if (!P.bulk) {
-                copy_rows(k + 1, nbuf);
-                __syncthreads();
-            }
-        }
-        if ((k + 1) % flush_every == 0) {   // every unit of the chunk has added its sums
-            flush();
-            __syncthreads();               // before the next chunk's units add again
         }
         if (tid == 0 && k + 2 < n_chunks) {
             fence_proxy_async();
