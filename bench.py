@@ -46,9 +46,11 @@ FLOP_PER_PAIR = 20
 MUFU_PER_PAIR = 4
 
 # DRAM traffic of one 64 x 64 x 1500 tile launch per trace of the panel, from an
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of the
-# full-size launch (1,048,576 traces, 24 MiB trace segments): 63.3 + 19.3 GB
-DRAM_BYTES_PER_TRACE_TILE64 = 82.6e9 / 1048576
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one launch over
+# 262,144 traces (a 1.6 GB panel, 24 MiB trace segments): 16.23 + 5.02 GB.  The
+# segment-major schedule reads each segment and re-adds the tile once per
+# segment, so the traffic grows with the trace count; scaled per trace.
+DRAM_BYTES_PER_TRACE_TILE64 = 21.25e9 / 262144
 
 
 def parse():
@@ -920,7 +922,7 @@ def main_ours(args):
                 "frac": alg_bytes / per_launch_s / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes,
                 "peak_source": hbm_src},
         "traffic": (DRAM_BYTES_PER_TRACE_TILE64 * N / 1e9) if T == 64 else None,
-        "traffic_unit": "GB per launch (ncu dram__bytes read+write of the full-size launch, scaled by traces)",
+        "traffic_unit": "GB per launch (ncu dram__bytes read+write of a 262,144-trace launch, scaled by traces)",
     }
 
     # ---- end to end through the public API with pinned host buffers
