@@ -1185,7 +1185,9 @@ def measure_case5(args):
         }
 
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    mufu_peak = 148 * 16 * sm_mhz * 1e6
+    mufu_peak, peak_src = measured_sfu_peak(int(os.environ.get("LOCAL_RANK", "0"))), "measured (MUFU-throughput kernel)"
+    if not mufu_peak:
+        mufu_peak, peak_src = 148 * 16 * sm_mhz * 1e6, "derived: 148 SMs x 16 MUFU/clk x median SM clock"
     mufu_per_pair = 8   # straight DSR 3 + AA 1 + curved legs 2 + VTI 2
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": len(results), "warmup": 0,
@@ -1201,7 +1203,7 @@ def measure_case5(args):
         "roofline": {"bound": "sfu", "unit": "Gop/s", "achieved": value * mufu_per_pair / 1e9,
                      "peak": mufu_peak / 1e9, "frac": value * mufu_per_pair / mufu_peak,
                      "per_pair": f"{mufu_per_pair} MUFU (DSR 3 + AA 1 + curved 2 + VTI 2)",
-                     "peak_source": "derived: 148 SMs x 16 MUFU/clk x median SM clock"},
+                     "peak_source": peak_src},
         "oracle_check": {"rel_l2_vs_fp64": err, "fold_bit_exact": fold_ok, "pillars": 64,
                          "sample": f"64 random output traces of tile {list(tiles[0])} x {NT5} samples against "
                                    f"every 32nd of its {int(ex.select(tiles[0]).numel())} selected traces "

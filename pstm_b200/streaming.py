@@ -227,8 +227,11 @@ class StreamingExecutor:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(self._copy)
+            # contiguous copies only: a strided destination would make torch run a
+            # copy kernel, which waits for SMs the migration kernel holds
             self._pool_amps[r0:r0 + n].copy_(sa[:n], non_blocking=True)
-            self._pool_geo[:, r0:r0 + n].copy_(self._stage_geo[k][:, :n], non_blocking=True)
+            for f in range(7):
+                self._pool_geo[f, r0:r0 + n].copy_(self._stage_geo[k][f, :n], non_blocking=True)
             e1.record(self._copy)
         self._stage_done[k] = e1
         self._copy_events.append((e0, e1))
