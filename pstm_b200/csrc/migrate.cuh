@@ -1,24 +1,22 @@
 // migrate.cuh -- gather-form Kirchhoff PSTM kernel for sm_100a.
 //
-// One CTA owns PB output pillars and, for each of them, a block of 512*R
-// output times.  It has 16 consumer warps (512 lanes) and one producer warp.
-// Consumer lane `tid` owns the R times t = t_block + tid + 512*r, so every
-// warp holds shallow and deep times alike and the work per warp is balanced.
-// Traces are streamed in chunks of C:
-//   staging  the producer warp copies the chunk's amplitude rows and packed
-//            FP64 geometry into shared memory with TMA bulk copies
-//            (cp.async.bulk + mbarrier), double-buffered;
-//   records  the producer warp gives every (pillar, trace) pair of a landed
-//            chunk a record in shared memory (FP64 geometry rounded once to
-//            FP32); the fold predicate is evaluated in FP64 and counted with
+// One CTA (16 warps, 512 lanes) owns PB output pillars and, for each of them,
+// a block of 512*R output times; lane `tid` owns the R times
+// t = t_block + tid + 512*r, so every warp holds shallow and deep times alike
+// and the work per warp is balanced.  A lane keeps the PB x R partial sums in
+// registers.  Traces are streamed in chunks of C:
+//   staging  the chunk's amplitude rows and packed FP64 geometry are copied
+//            into shared memory by TMA bulk copies (cp.async.bulk + mbarrier),
+//            double-buffered, so chunk k+1 lands while chunk k is processed;
+//   records  every (pillar, trace) pair of the next chunk gets a record in
+//            shared memory (FP64 geometry rounded once to FP32); the fold
+//            predicate is evaluated in FP64 and counted with warp match /
 //            ballot + popc;
-//   pairs    every consumer lane walks the records of its current chunk
-//            (warp-uniform broadcast reads) and, for each of its R times,
-//            evaluates traveltime, sample index, linear interpolation (from
-//            shared memory) and weights, with warp-uniform skips instead of
+//   pairs    every lane walks the records of the current chunk (warp-uniform
+//            broadcast reads) and, for each of its R times, evaluates
+//            traveltime, sample index, linear interpolation (from shared
+//            memory) and weights, with warp-uniform skips instead of
 //            divergent branches.
-// Producer and consumers meet only at mbarriers (copies landed, records built,
-// chunk consumed), never at a CTA-wide barrier inside the trace loop.
 // Chunk partials are added into FP32 partial sums in shared memory (with
 // their TwoSum rounding errors kept apart when compensated accumulation is
 // on), which are added into the caller's image (+=) every 16 chunks and at
@@ -46,8 +44,7 @@
 
 namespace pstm {
 
-constexpr int kThreads = 512;        // consumer lanes per CTA = output times per r
-constexpr int kCtaThreads = kThreads + 32;   // + one producer warp (copies and records)
+constexpr int kThreads = 512;        // lanes per CTA = output times per r
 constexpr int kMaxChunk = 32;        // traces per chunk, upper bound
 constexpr int kGeoDoubles = 8;       // packed geometry per trace: sx sy rx ry mx my w 0
 constexpr int kWaitIters = 1 << 20;  // default bound of every mbarrier wait loop (KParams::wait_iters)
@@ -140,31 +137,16 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
-    return done != 0;
-}
 // Bounded wait for the mbarrier phase with the given parity: at most `iters`
 // polls (each a potentially blocking try_wait); false = gave up.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int iters) {
-    for (int i = 0; i < iters; ++i)
-        if (mbar_try(bar, parity)) return true;
-    return false;
-}
-// The same, giving up early once another warp of the CTA has raised `abort`
-// (its own wait ran out); the result is the same for every lane of the warp.
-__device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity, int iters, const volatile int *abort) {
-    bool ok = false;
     for (int i = 0; i < iters; ++i) {
-        if (mbar_try(bar, parity)) { ok = true; break; }
-        if (*abort) break;
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
     }
-    return __all_sync(0xffffffffu, ok);
+    return false;
 }
 
 // ---------------------------------------------------------------- per-time state
@@ -480,11 +462,8 @@ struct CtaShared {
     int pid[kMaxPB];
     int fold[kMaxPB];
     int rank[kMaxPB][kMaxChunk];
-    unsigned long long bar[2];    // chunk copies landed (TMA transaction count)
-    unsigned long long rbar[2];   // chunk records built (the producer warp's 32 lanes)
-    unsigned long long ebar[2];   // chunk consumed (one arrival per consumer warp)
+    unsigned long long bar[2];
     long long item;
-    int abort;                    // a bounded wait of some warp ran out
 };
 
 // Migrates one item.  `chunk_base` counts the chunks this CTA staged before
@@ -527,11 +506,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         s_ox[tid] = ok ? (P.xg ? P.xg[p] : P.xa[ix]) : 0.0;
         s_oy[tid] = ok ? (P.yg ? P.yg[p] : P.ya[iy]) : 0.0;
     }
-    const bool producer = tid >= kThreads;   // the last warp: copies and records
     const uint32_t bar0 = smem_u32(&sh.bar[0]), bar1 = smem_u32(&sh.bar[1]);
-    const uint32_t rbar0 = smem_u32(&sh.rbar[0]), rbar1 = smem_u32(&sh.rbar[1]);
-    const uint32_t ebar0 = smem_u32(&sh.ebar[0]), ebar1 = smem_u32(&sh.ebar[1]);
-    const volatile int *const abort_flag = &sh.abort;
     const int t_lane = it.tblock * (kThreads * R) + tid;   // this thread's times: t_lane + r * kThreads
 
     // hot-loop constants in registers
@@ -551,8 +526,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     const int64_t n_chunks = (it.n_traces + C - 1) / C;
     const int flush_every = P.flush_every;
 
-    if (!producer)
-        for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
+    for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
 
     // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
     // rows when they are 16-byte aligned) into buffer b
@@ -655,22 +629,27 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             if constexpr (HAS_C) reinterpret_cast<float4 *>(recA + 2 * RECS)[ri] = Cc;
         }
     };
-    // amplitude rows not 16-byte aligned (no TMA bulk copy): plain copy by the producer warp
+    // amplitude rows not 16-byte aligned (no TMA bulk copy): plain cooperative copy by all threads
     auto copy_rows = [&](int64_t k, int b) {
         const int64_t c0 = k * C;
         const int cmax = (int)min((int64_t)C, it.n_traces - c0);
-        unsigned char *dst = amp_base + b * amp_bytes;
-        for (int rr = 0; rr < cmax; ++rr) {
-            const int64_t g0 = (c0 + rr) * P.amp_stride;
-            for (int ii = lane; ii < P.ns; ii += 32) {
+        {
+            unsigned char *dst = amp_base + b * amp_bytes;
+            const unsigned char *src = it.amps;
+            for (int e = tid; e < cmax * P.ns; e += kThreads) {
+                const int rr = e / P.ns, ii = e - rr * P.ns;
+                const int64_t gi = (c0 + rr) * P.amp_stride + ii;
                 if (P.elem == 4)
-                    reinterpret_cast<float *>(dst + rr * row_bytes)[ii] =
-                        reinterpret_cast<const float *>(it.amps)[g0 + ii];
+                    reinterpret_cast<float *>(dst + rr * row_bytes)[ii] = reinterpret_cast<const float *>(src)[gi];
                 else
                     reinterpret_cast<unsigned short *>(dst + rr * row_bytes)[ii] =
-                        reinterpret_cast<const unsigned short *>(it.amps)[g0 + ii];
+                        reinterpret_cast<const unsigned short *>(src)[gi];
             }
         }
+    };
+    auto build_records = [&](int64_t k, int b) {   // every pillar (warp q < PB) and the row copy
+        if (warp < PB) pillar_records(k, b, warp);
+        if (!P.bulk) copy_rows(k, b);
     };
 
     // add this lane's FP32 partial sums into the FP64 (or FP32) image and clear them
@@ -704,88 +683,30 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         }
     };
 
-    __syncthreads();   // pillars known, partial sums clear
-    // Chunk k of this item is the CTA's chunk g = chunk_base + k: it uses buffer
-    // g & 1 and completes one phase, of parity (g >> 1) & 1, of each of that
-    // buffer's three mbarriers: copies landed (bar), records built (rbar),
-    // consumed by all 16 consumer warps (ebar).  The producer warp issues the
-    // copies of chunk k + 2 once chunk k is consumed and builds its records as
-    // soon as they land, so consumer warps wait neither for each other nor for
-    // record building; a fast warp runs at most two chunks ahead of the slowest.
-    const int64_t cb = chunk_base;
-    const int b0 = (int)(cb & 1);
+    __syncthreads();   // pillars known
+    // chunk k of this item is the CTA's chunk g = chunk_base + k: buffer g & 1,
+    // mbarrier phase parity (g >> 1) & 1
+    const int b0 = (int)(chunk_base & 1);
     const int wait_iters = P.wait_iters;
-    if (producer) {
-        // (fault injection: with inject_stall the first copies are never issued,
-        // so nothing completes their phase and the bounded wait for them runs out)
-        if (lane == 0 && !P.inject_stall) {
-            if (cb > 0) fence_proxy_async();   // the previous item's reads of the buffers
-            if (n_chunks > 0) issue_chunk(0, b0);
-            if (n_chunks > 1) issue_chunk(1, b0 ^ 1);
-        }
-        int64_t issued = P.inject_stall ? 0 : min(n_chunks, (int64_t)2), landed = 0;
-        // records of chunk j once its copies have landed
-        auto build = [&](int64_t j) -> bool {
-            const int64_t g = cb + j;
-            const int b = (int)(g & 1);
-            if (!mbar_wait_warp(b ? bar1 : bar0, (uint32_t)((g >> 1) & 1), wait_iters, abort_flag)) return false;
-            landed = j + 1;
-            if (!P.bulk) copy_rows(j, b);
-#pragma unroll 1
-            for (int q = 0; q < PB; ++q) pillar_records(j, b, q);
-            __syncwarp();
-            mbar_arrive(b ? rbar1 : rbar0);
-            return true;
-        };
-        bool ok = true;
-        if (n_chunks > 0) ok = build(0);
-        if (ok && n_chunks > 1) ok = build(1);
-#pragma unroll 1
-        for (int64_t k = 0; ok && k + 2 < n_chunks; ++k) {
-            const int64_t g = cb + k;
-            const int b = (int)(g & 1);
-            ok = mbar_wait_warp(b ? ebar1 : ebar0, (uint32_t)((g >> 1) & 1), wait_iters, abort_flag);
-            if (!ok) break;
-            if (lane == 0) {
-                fence_proxy_async();   // the consumers' reads of the buffer come first
-                issue_chunk(k + 2, b);
-            }
-            issued = k + 3;
-            __syncwarp();
-            ok = build(k + 2);
-        }
-        if (!ok && lane == 0) {
-            atomicOr(P.err, (int)KERR_WAIT_TIMEOUT);
-            sh.abort = 1;
-        }
-        chunk_base += n_chunks;
-        __syncthreads();   // every warp is done with this item
-        if (sh.abort) {
-            // a copy never completed: drain what may still be in flight, leave
-            if (lane == 0)
-                for (int64_t j = landed; j < issued; ++j)
-                    mbar_wait(((cb + j) & 1) ? bar1 : bar0, (uint32_t)(((cb + j) >> 1) & 1), wait_iters);
-            __syncthreads();
-            return false;
-        }
-        return true;
+    // (fault injection: with inject_stall the first copies are never issued, so
+    // nothing completes their phase and the bounded wait below runs out)
+    if (tid == 0 && !P.inject_stall) {
+        if (chunk_base > 0) fence_proxy_async();   // the previous item's reads of the buffers
+        if (n_chunks > 0) issue_chunk(0, b0);
+        if (n_chunks > 1) issue_chunk(1, b0 ^ 1);
     }
+    bool aborted = false;
+    if (n_chunks > 0) {
+        const bool ok = mbar_wait(b0 ? bar1 : bar0, (uint32_t)((chunk_base >> 1) & 1), wait_iters);
+        if (__syncthreads_or(!ok)) aborted = true;
+        else build_records(0, b0);
+    }
+    __syncthreads();
 
-#pragma unroll 1
-    for (int64_t k = 0; k < n_chunks; ++k) {
+    for (int64_t k = 0; k < n_chunks && !aborted; ++k) {
         const int64_t c0 = k * C;
-        const int64_t g = cb + k;
+        const int64_t g = chunk_base + k;
         const int buf = (int)(g & 1);
-        const uint32_t par = (uint32_t)((g >> 1) & 1);
-        // records built (and, for the memory order of the copied rows, the copies landed)
-        if (!mbar_wait_warp(buf ? rbar1 : rbar0, par, wait_iters, abort_flag) ||
-            !mbar_wait_warp(buf ? bar1 : bar0, par, wait_iters, abort_flag)) {
-            if (lane == 0) {
-                atomicOr(P.err, (int)KERR_WAIT_TIMEOUT);
-                sh.abort = 1;
-            }
-            break;
-        }
         const float4 *recA = reinterpret_cast<const float4 *>(rec_base + buf * REC_BYTES);
         const unsigned char *ampb = amp_base + buf * amp_bytes;
 
@@ -1026,14 +947,34 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
             }
         }
 
+        // ---------------- records of chunk k+1 (its copy was issued a chunk ago)
+        bool timeout = false;
+        if (k + 1 < n_chunks) {
+            const int nb = buf ^ 1;
+            timeout = !mbar_wait(nb ? bar1 : bar0, (uint32_t)(((g + 1) >> 1) & 1), wait_iters);
+            if (!timeout) build_records(k + 1, nb);
+        }
         if ((k + 1) % flush_every == 0) flush();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(buf ? ebar1 : ebar0);   // this warp is done with buffer `buf`
+        if (__syncthreads_or(timeout)) {   // also: buffer `buf` is free again
+            aborted = true;
+            break;
+        }
+        if (tid == 0 && k + 2 < n_chunks) {
+            fence_proxy_async();
+            issue_chunk(k + 2, buf);
+        }
     }
 
     chunk_base += n_chunks;
-    __syncthreads();   // every warp is done with this item; the fold counts are final
-    if (sh.abort) {    // a copy never completed: the producer drains, nobody flushes
+    if (aborted) {
+        // a copy never completed: report, drain what may still be in flight, leave
+        if (tid == 0) {
+            atomicOr(P.err, (int)KERR_WAIT_TIMEOUT);
+            mbar_wait(bar0, 0, wait_iters);
+            mbar_wait(bar0, 1, wait_iters);
+            mbar_wait(bar1, 0, wait_iters);
+            mbar_wait(bar1, 1, wait_iters);
+        }
         __syncthreads();
         return false;
     }
@@ -1067,24 +1008,20 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     return true;
 }
 
-// Initialises the staging mbarriers of a CTA (two buffers: copies landed,
-// records built by the producer warp's 32 lanes, consumed by the 16 consumer warps).
+// Initialises the two staging mbarriers of a CTA.
 __device__ __forceinline__ void init_barriers(CtaShared &sh) {
     if (threadIdx.x == 0) {
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(smem_u32(&sh.bar[b]), 1);
-            mbar_init(smem_u32(&sh.rbar[b]), 32);
-            mbar_init(smem_u32(&sh.ebar[b]), kThreads / 32);
-        }
-        sh.abort = 0;
+        mbar_init(smem_u32(&sh.bar[0]), 1);
+        mbar_init(smem_u32(&sh.bar[1]), 1);
         fence_barrier_init();
     }
 }
 
 // One CTA per (pillar block, time block) of one tile.
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
-__global__ void __launch_bounds__(kCtaThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1)
 migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
+    static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ CtaShared sh;
     init_barriers(sh);
@@ -1109,7 +1046,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
 // block) of P.image / P.fold, numbered segment by segment; an item finds its
 // segment by binary search in the segments' inclusive prefix counts.
 template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
-__global__ void __launch_bounds__(kCtaThreads, 1)
+__global__ void __launch_bounds__(kThreads, 1)
 migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const BinWork *__restrict__ bins,
                           int n_bins, unsigned long long *work_counter, const ScatterWork sw) {
     extern __shared__ __align__(128) unsigned char smem[];

@@ -40,7 +40,7 @@ static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L
         static SmemOptIn opt_in;   // per instantiation
         cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
         if (e != cudaSuccess) return e;
-        kern<<<L.grid, kCtaThreads, L.smem, L.stream>>>(P, Pg);
+        kern<<<L.grid, kThreads, L.smem, L.stream>>>(P, Pg);
         return cudaGetLastError();
     }
     auto kern = migrate_persistent_kernel<TT, AMP, VEL3D, EXACT, W2>;
@@ -54,7 +54,7 @@ static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCtaThreads, L.smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, L.smem);
         if (e != cudaSuccess) return e;
         ctas = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
     }
@@ -62,7 +62,7 @@ static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L
         if (L.ctas_out) *L.ctas_out = ctas;
         return cudaSuccess;
     }
-    kern<<<ctas, kCtaThreads, L.smem, L.stream>>>(P, Pg, L.bins, L.n_bins, L.counter, L.scatter);
+    kern<<<ctas, kThreads, L.smem, L.stream>>>(P, Pg, L.bins, L.n_bins, L.counter, L.scatter);
     return cudaGetLastError();
 }
 
