@@ -177,39 +177,11 @@ struct PtState {
     double c1B, e2B2;      // EXACT, VTI kinds: (1+2eta) / (v dt)^2, 2 eta / (v dt)^4
 };
 
-// The table entries of one (pillar, time): what load_states reads from
-// global memory, fetched apart from the arithmetic on them so that the gather
-// loop can fetch the next (pillar, time)'s entries while it works on the
-// current one.
-struct RawState {
-    float4 a, b, tab;
-    double A, V, B, eta;
-    bool valid;
-};
-
 template <int TT, bool EXACT>
-__device__ __forceinline__ void fetch_state(const KParams &P, int p, int t, RawState &w) {
-    w.valid = t < P.nt;
-    const int tc = w.valid ? t : P.nt - 1;
-    w.a = P.ttime[2 * tc];
-    w.b = P.ttime[2 * tc + 1];
-    w.A = EXACT ? P.ttimeA[tc] : 0.0;
-    w.V = 0.0;
-    if constexpr (EXACT && (TT == TT_CURVED || TT == TT_CURVED_VTI)) w.V = P.ttimeV[tc];
-    const int64_t ti = (P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc;
-    w.tab = P.ttab[ti];
-    w.B = EXACT ? P.btab[ti] : 0.0;
-    w.eta = 0.0;
-    if constexpr (EXACT && (TT == TT_VTI || TT == TT_CURVED_VTI)) {
-        w.eta = P.eta_const;
-        if (P.eta) w.eta = P.eta3d ? P.eta[(int64_t)p * P.nt + tc] : P.eta[tc];
-    }
-}
-
-template <int TT, bool EXACT>
-__device__ __forceinline__ void derive_states(const KParams &P, const RawState &w, TimeState &ts, PtState &s) {
-    const bool valid = w.valid;
-    const float4 a = w.a, b = w.b;
+__device__ __forceinline__ void load_states(const KParams &P, int p, int t, TimeState &ts, PtState &s) {
+    const bool valid = t < P.nt;
+    const int tc = valid ? t : P.nt - 1;
+    const float4 a = P.ttime[2 * tc], b = P.ttime[2 * tc + 1];
     ts.t0h2 = a.x;
     ts.Kt = a.y;
     ts.tg = a.z;
@@ -220,13 +192,14 @@ __device__ __forceinline__ void derive_states(const KParams &P, const RawState &
     ts.tzero = b.w != 0.f;
     ts.tz = b.w >= 2.f;
     ts.tz_in = b.w == 2.f;
-    ts.A = w.A;
+    ts.A = EXACT ? P.ttimeA[tc] : 0.0;
     ts.vz64 = ts.vz2_64 = 0.0;
     if constexpr (EXACT && (TT == TT_CURVED || TT == TT_CURVED_VTI)) {
-        ts.vz64 = w.V;
+        ts.vz64 = P.ttimeV[tc];
         ts.vz2_64 = ts.vz64 * ts.vz64;
     }
-    const float4 tab = w.tab;
+    const int64_t ti = (P.vel3d || P.eta3d) ? (int64_t)p * P.nt + tc : tc;
+    const float4 tab = P.ttab[ti];
     s.iv2 = tab.x;
     s.iv2r = tab.x;
     s.ap = valid ? tab.y : -1.f;   // a time past the tile end is never inside the aperture
@@ -258,19 +231,14 @@ __device__ __forceinline__ void derive_states(const KParams &P, const RawState &
         s.c1 = 1.f + 2.f * tab.w;
         s.e2 = 2.f * tab.w * tab.x;
     }
-    s.B = w.B;
+    s.B = EXACT ? P.btab[ti] : 0.0;
     s.c1B = s.e2B2 = 0.0;
     if constexpr (EXACT && (TT == TT_VTI || TT == TT_CURVED_VTI)) {
-        s.c1B = (1.0 + 2.0 * w.eta) * s.B;
-        s.e2B2 = 2.0 * w.eta * s.B * s.B;
+        double eta = P.eta_const;
+        if (P.eta) eta = P.eta3d ? P.eta[(int64_t)p * P.nt + tc] : P.eta[tc];
+        s.c1B = (1.0 + 2.0 * eta) * s.B;
+        s.e2B2 = 2.0 * eta * s.B * s.B;
     }
-}
-
-template <int TT, bool EXACT>
-__device__ __forceinline__ void load_states(const KParams &P, int p, int t, TimeState &ts, PtState &s) {
-    RawState w;
-    fetch_state<TT, EXACT>(P, p, t, w);
-    derive_states<TT, EXACT>(P, w, ts, s);
 }
 
 // FP64 traveltime in samples (the EXACT path of the curved and VTI kinds) of
@@ -727,8 +695,6 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
         if (n_chunks > 0) issue_chunk(0, b0);
         if (n_chunks > 1) issue_chunk(1, b0 ^ 1);
     }
-    RawState nxt;   // table entries of the (pillar, time) the pair loop takes next
-    fetch_state<TT, EXACT>(P, s_pid[0] < 0 ? 0 : s_pid[0], t_lane, nxt);
     bool aborted = false;
     if (n_chunks > 0) {
         const bool ok = mbar_wait(b0 ? bar1 : bar0, (uint32_t)((chunk_base >> 1) & 1), wait_iters);
@@ -748,27 +714,16 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
 #pragma unroll 1
         for (int q = 0; q < PB; ++q) {
             const int p = s_pid[q];
+            if (p < 0) continue;
             const float4 *A_q = recA + q * kMaxChunk;
             const float dl = A_q[lane].x;   // this lane's slot of the sorted distances
             const int vt = tid;             // the partial sums of this thread's times
 #pragma unroll 1
             for (int r = 0; r < R; ++r) {
                 const int t = t_lane + r * kThreads;
-                const RawState w = nxt;
-                {   // the next (pillar, time)'s table entries, in flight during this one's pairs
-                    // (after the last, the first of the next chunk: the same pillars and times)
-                    int q2 = q, r2 = r + 1;
-                    if (r2 == R) {
-                        r2 = 0;
-                        q2 = q + 1 == PB ? 0 : q + 1;
-                    }
-                    const int p2 = s_pid[q2];
-                    fetch_state<TT, EXACT>(P, p2 < 0 ? 0 : p2, t_lane + r2 * kThreads, nxt);
-                }
-                if (p < 0) continue;
                 TimeState ts;
                 PtState s;
-                derive_states<TT, EXACT>(P, w, ts, s);
+                load_states<TT, EXACT>(P, p, t, ts, s);
                 // records inside the aperture of some lane: a prefix of length n;
                 // records with no lane in its taper band: a prefix of length n0
                 const float apw = __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(s.ap)));
