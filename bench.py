@@ -1176,6 +1176,7 @@ def measure_case5(args):
             "pool_gb": sx.S * sx.B * (NS5 * 2 + 56) / 1e9, "blocks_loaded": rep_s.misses, "block_hits": rep_s.hits,
             "h2d_gb": rep_s.h2d_bytes / 1e9, "copy_ms": rep_s.copy_ms, "kernel_ms": rep_s.kernel_ms,
             "wall_ms": rep_s.wall_s * 1e3, "exposed_ms": rep_s.exposed_ms,
+            "first_load_ms": rep_s.first_load_ms, "copy_overlap_ms": rep_s.copy_overlap_ms,
             "overlapped_copy_fraction": rep_s.overlapped_copy_fraction,
             "h2d_gbs": rep_s.h2d_bytes / max(rep_s.copy_ms, 1e-9) / 1e6,
             "value": sum(r.pairs for r in results if r.tile == st_tile) / (rep_s.wall_s or 1e-9),

@@ -95,6 +95,8 @@ class StreamReport:
     wall_s: float = 0.0
     kernel_ms: float = 0.0         # sum of the migration calls' CUDA-event times
     copy_ms: float = 0.0           # sum of the block copies' CUDA-event times (copy stream)
+    copy_overlap_ms: float = 0.0   # the part of copy_ms during which a migration kernel ran
+    first_load_ms: float = 0.0     # run start -> first kernel start: the first pass's gather and copies
     h2d_bytes: int = 0
     hits: int = 0
     misses: int = 0
@@ -106,10 +108,29 @@ class StreamReport:
 
     @property
     def overlapped_copy_fraction(self) -> float:
-        """Share of the copy time that ran under the kernels (1 - exposed / copy, clipped)."""
+        """Share of the copy time that ran while a migration kernel ran, from the
+        CUDA events of both streams (timestamps on one device clock)."""
         if self.copy_ms <= 0:
             return 1.0
-        return float(min(1.0, max(0.0, 1.0 - self.exposed_ms / self.copy_ms)))
+        return float(min(1.0, self.copy_overlap_ms / self.copy_ms))
+
+
+def overlap_ms(intervals, cover) -> float:
+    """Total length of the parts of ``intervals`` (start, end) that lie inside
+    the union of ``cover`` (start, end)."""
+    merged: list[list[float]] = []
+    for a, b in sorted(cover):
+        if merged and a <= merged[-1][1]:
+            merged[-1][1] = max(merged[-1][1], b)
+        else:
+            merged.append([a, b])
+    tot = 0.0
+    for a, b in intervals:
+        for c, d in merged:
+            lo, hi = max(a, c), min(b, d)
+            if hi > lo:
+                tot += hi - lo
+    return tot
 
 
 class StreamingExecutor:
@@ -260,6 +281,9 @@ class StreamingExecutor:
         self._copy_events = []
         t0 = time.perf_counter()
         compute = torch.cuda.current_stream()
+        origin = torch.cuda.Event(enable_timing=True)   # the common time origin of both streams' events
+        origin.record(compute)
+        self._copy.wait_event(origin)
         nt = len(self.t_axis_ms)
         cur_tile, timg, tfold, out, vel = None, None, None, None, None
         pending = []
@@ -302,6 +326,10 @@ class StreamingExecutor:
             pr.kernel_ms = e0.elapsed_time(e1)
         rep.kernel_ms = sum(p.kernel_ms for p in rep.passes)
         rep.copy_ms = sum(a.elapsed_time(b) for a, b in self._copy_events)
+        rel = lambda e: origin.elapsed_time(e)
+        kern = [(rel(e0), rel(e1)) for _, e0, e1 in pending]
+        rep.copy_overlap_ms = overlap_ms([(rel(a), rel(b)) for a, b in self._copy_events], kern)
+        rep.first_load_ms = kern[0][0] if kern else 0.0
         rep.h2d_bytes = sum(p.h2d_bytes for p in rep.passes)
         rep.misses = sum(p.loaded for p in rep.passes)
         rep.hits = sum(len(p.blocks) for p in rep.passes) - rep.misses

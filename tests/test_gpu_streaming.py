@@ -52,6 +52,7 @@ def test_streamed_grid_matches_resident_call_and_oracle(dtype, cuda_kernel_facto
     assert len(rep.passes) > 9                  # tiles split into several passes
     assert rep.misses > ex.S                    # blocks were evicted and reloaded
     assert rep.h2d_bytes > 0 and rep.kernel_ms > 0
+    assert 0.0 <= rep.copy_overlap_ms <= rep.copy_ms + 1e-3 and rep.first_load_ms >= 0.0
     np.testing.assert_array_equal(fold.cpu().numpy(), ref.fold.cpu().numpy())
     assert float(ref.image.abs().max()) > 0
     assert rel_l2(img.cpu().numpy(), ref.image.cpu().numpy()) <= 1e-6

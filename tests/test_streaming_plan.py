@@ -49,3 +49,12 @@ def test_pool_runs_map_rows_to_their_traces():
     back = np.array([block_of_slot[r // B] * B + r % B for r in rows])
     want = np.concatenate([np.arange(a, b) for a, b in runs])
     np.testing.assert_array_equal(np.sort(back), want)
+
+
+def test_overlap_of_copies_with_kernels():
+    from pstm_b200.streaming import overlap_ms
+    kernels = [(10.0, 20.0), (18.0, 30.0), (40.0, 50.0)]      # union [10, 30] and [40, 50]
+    copies = [(0.0, 12.0), (25.0, 45.0), (50.0, 60.0), (31.0, 39.0)]
+    assert overlap_ms(copies, kernels) == 2.0 + (5.0 + 5.0) + 0.0 + 0.0
+    assert overlap_ms([], kernels) == 0.0
+    assert overlap_ms(copies, []) == 0.0
