@@ -16,10 +16,11 @@ the GPU as the cache:
   those ranges where the blocks lie in the pool
   (``CudaKernel.migrate_tile_runs``): the pool is one device panel;
 * while the kernel migrates one pass (a tile, or the part of a tile whose
-  blocks fit in half the pool), the host gathers the next pass's missing
-  blocks into pinned staging buffers and copies them to their slots on a
-  second stream, so host->device traffic overlaps the kernel.  A copy into
-  a slot waits for the last kernel that read that slot.
+  blocks fit in half the pool), host threads gather the next pass's missing
+  blocks into a ring of pinned staging buffers, several blocks at a time, and
+  the main thread copies each gathered block to its slot on a second stream,
+  so host->device traffic overlaps the kernel.  A copy into a slot waits for
+  the last kernel that read that slot.
 
 So panels larger than HBM run, and HBM holds only the pool.  The result is
 the resident executor's up to the order of floating-point additions (a tile
@@ -28,7 +29,8 @@ split over several passes adds each pass into its image and fold).
 from __future__ import annotations
 
 import time
-from collections import OrderedDict
+from collections import OrderedDict, deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -146,7 +148,7 @@ class StreamingExecutor:
     def __init__(self, kernel, traces, x_axis, y_axis, t_axis_ms, velocity, config,
                  kernel_type: str = "straight_ray", tile: int = 64, block_traces: int = 65536,
                  pool_blocks: int | None = None, pool_bytes: int | None = None,
-                 column_width_m: float | None = None):
+                 column_width_m: float | None = None, gather_threads: int = 4):
         import torch
         from .spatial import MidpointIndex
         self.torch = torch
@@ -189,10 +191,14 @@ class StreamingExecutor:
         rows = self.S * self.B
         self._pool_amps = torch.empty((rows, self.ns), dtype=tdt, device="cuda")
         self._pool_geo = torch.zeros((7, rows), dtype=torch.float64, device="cuda")
-        self._stage_amps = [torch.empty((self.B, self.ns), dtype=tdt, pin_memory=True) for _ in range(2)]
-        self._stage_geo = [torch.empty((7, self.B), dtype=torch.float64, pin_memory=True) for _ in range(2)]
-        self._stage_done = [None, None]   # copy-stream events of the staging buffers' last copies
+        # a ring of pinned staging buffers, one host gather thread each
+        self.n_stage = max(2, int(gather_threads))
+        self._stage_amps = [torch.empty((self.B, self.ns), dtype=tdt, pin_memory=True) for _ in range(self.n_stage)]
+        self._stage_geo = [torch.empty((7, self.B), dtype=torch.float64, pin_memory=True)
+                           for _ in range(self.n_stage)]
+        self._stage_done = [None] * self.n_stage   # copy-stream events of the staging buffers' last copies
         self._stage_next = 0
+        self._gather_pool = ThreadPoolExecutor(max_workers=self.n_stage)
         self._copy = torch.cuda.Stream()
         self._slot_of: "OrderedDict[int, int]" = OrderedDict()   # block -> slot, least recent first
         self._free = list(range(self.S))
@@ -226,21 +232,25 @@ class StreamingExecutor:
                 return slot
         raise RuntimeError("the device pool cannot hold two passes' blocks; give it more slots")
 
-    def _load(self, blk: int, keep: set) -> int:
+    def _gather(self, blk: int, k: int) -> int:
+        """Host side of a block load: its traces (midpoint order) into staging
+        buffer k (runs in a gather thread; NumPy releases the GIL here)."""
         torch = self.torch
-        slot = self._free.pop() if self._free else self._victim(keep)
         idx = self.index.order[blk * self.B:(blk + 1) * self.B]
         n = len(idx)
-        k = self._stage_next
-        self._stage_next ^= 1
-        if self._stage_done[k] is not None:
-            self._stage_done[k].synchronize()      # the staging buffer's previous copy has left it
         sa = self._stage_amps[k]
         sa_np = (sa.view(torch.int16) if sa.dtype == torch.bfloat16 else sa).numpy()
         np.take(self._host_amps, idx, axis=0, out=sa_np[:n])
         sg = self._stage_geo[k].numpy()
         for i, a in enumerate(self._host_geo):
             np.take(a, idx, out=sg[i, :n])
+        return n
+
+    def _copy_in(self, blk: int, slot: int, k: int, n: int) -> int:
+        """Device side of a block load: staging buffer k -> the block's slot on
+        the copy stream, after the last kernel that read the slot."""
+        torch = self.torch
+        sa = self._stage_amps[k]
         r0 = slot * self.B
         with torch.cuda.stream(self._copy):
             if self._slot_reader[slot] is not None:
@@ -261,13 +271,32 @@ class StreamingExecutor:
         return n * (self.ns * self._host_amps.itemsize + 7 * 8)
 
     def _ensure(self, blocks, keep: set) -> tuple[int, int]:
+        """Loads the blocks missing from the pool: slots are chosen in order
+        (least recently used first), gathers run n_stage at a time in host
+        threads, and each gathered block is copied as soon as it is ready."""
         loaded = nbytes = 0
+        inflight: deque = deque()
+
+        def finish():
+            nonlocal nbytes
+            fut, blk, slot, k = inflight.popleft()
+            nbytes += self._copy_in(blk, slot, k, fut.result())
+
         for blk in blocks:
             if blk in self._slot_of:
                 self._slot_of.move_to_end(blk)
                 continue
-            nbytes += self._load(blk, keep)
+            slot = self._free.pop() if self._free else self._victim(keep)
+            if len(inflight) == self.n_stage:
+                finish()
+            k = self._stage_next
+            self._stage_next = (k + 1) % self.n_stage
+            if self._stage_done[k] is not None:
+                self._stage_done[k].synchronize()      # the staging buffer's previous copy has left it
+            inflight.append((self._gather_pool.submit(self._gather, blk, k), blk, slot, k))
             loaded += 1
+        while inflight:
+            finish()
         return loaded, nbytes
 
     # ------------------------------------------------------------- running
