@@ -29,6 +29,7 @@ split over several passes adds each pass into its image and fold).
 from __future__ import annotations
 
 import time
+import weakref
 from collections import OrderedDict, deque
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
@@ -199,6 +200,7 @@ class StreamingExecutor:
         self._stage_done = [None] * self.n_stage   # copy-stream events of the staging buffers' last copies
         self._stage_next = 0
         self._gather_pool = ThreadPoolExecutor(max_workers=self.n_stage)
+        weakref.finalize(self, self._gather_pool.shutdown, wait=False)
         self._copy = torch.cuda.Stream()
         self._slot_of: "OrderedDict[int, int]" = OrderedDict()   # block -> slot, least recent first
         self._free = list(range(self.S))
