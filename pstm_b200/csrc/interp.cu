@@ -50,6 +50,10 @@ __device__ inline R sample_at(const unsigned char *row, int64_t i) {
 // sincospi in the interpolation arithmetic: FP64, or FP32 on the fast path.
 __device__ inline void sincospi_r(double x, double *s, double *c) { sincospi(x, s, c); }
 __device__ inline void sincospi_r(float x, float *s, float *c) { sincospif(x, s, c); }
+// 1/x in the interpolation arithmetic: the hardware approximation refined by
+// one Newton step in FP64 (~1 ulp), the approximation itself in FP32.
+__device__ inline double rcp_r(double x) { return rcp_newton(x); }
+__device__ inline float rcp_r(float x) { return rcp_approx(x); }
 
 // Nearest, Catmull-Rom cubic and linear interpolation at fractional index t
 // (0 <= t < ns - 1 is checked by the caller); linear also serves the wide
@@ -84,8 +88,9 @@ __device__ R interpolate_narrow(const unsigned char *row, int ns, double t, int 
 // The taps need sin(pi x) and the sine or cosine of pi x / HW at x = frac - k,
 // k = -HW+1 .. HW.  Since sin(pi (frac - k)) = (-1)^k sin(pi frac) and the
 // window angle pi (frac - k) / HW moves by pi / HW from one tap to the next,
-// one sincospi of frac and a chain of window angles carried by rotations
-// through (cos_d, sin_d) = (cos, sin)(pi / HW) give every weight.  A rotation
+// a chain of window angles carried by rotations through (cos_d, sin_d) =
+// (cos, sin)(pi / HW) gives every weight, and the factor sin(pi frac) common
+// to all taps cancels in the normalisation.  A rotation
 // adds about one rounding of a unit-sized value per tap (absolute 1e-15 after
 // 16 taps), harmless where the window enters as 0.5 (1 + cos).  Lanczos
 // divides sin(pi x / HW) by x, so it needs that sine accurate relative to its
@@ -103,50 +108,57 @@ __device__ R interpolate_wide(const unsigned char *row, int ns, double t, R cos_
     }
     const int64_t ic = LANCZOS ? (int64_t)t : (int64_t)(t + 0.5);
     const R frac = (R)(t - (double)ic);
-    const R pi = (R)M_PI;
-    R s_f, c_f;
-    sincospi_r(frac, &s_f, &c_f);
+    // On a sample (|x| < 1e-10 at a tap: the tap's weight is 1 and the others'
+    // sin(pi x) factors vanish) the interpolant is that sample.
+    if (fabs(frac) < R(1e-10)) return sample_at<AMP, R>(row, ic);
+    if (LANCZOS && fabs(frac - R(1)) < R(1e-10)) return sample_at<AMP, R>(row, ic + 1);
+    // The factors common to every tap cancel in the normalisation, so they are
+    // left out: sinc weights sin(pi x_k) / (pi x_k) * 0.5 (1 + cos w_k) with
+    // sin(pi x_k) = (-1)^k sin(pi frac) become (-1)^k (1 + cos w_k) / x_k, and
+    // Lanczos weights sin(pi x_k) sin(pi x_k / HW) HW / (pi^2 x_k^2) become
+    // (-1)^k sin(pi x_k / HW) / x_k^2; one reciprocal per tap, no division.
     R acc = R(0), norm = R(0);
-    auto tap = [&](int k, R s_k, R s_w, R c_w) {
+    auto tap = [&](int k, R sg, R s_w, R c_w) {
         const int64_t i = ic + k;
         if (i < 0 || i >= ns) return;   // (sinc rounds to the nearest sample: ic + HW can reach ns)
         const R x = frac - (R)k;
+        const R rx = rcp_r(x);
         R w;
-        if (LANCZOS) w = fabs(x) < R(1e-10) ? R(1) : (fabs(x) >= R(HW) ? R(0) : (s_k * s_w * R(HW)) / (pi * pi * x * x));
-        else w = (fabs(x) < R(1e-10) ? R(1) : s_k / (pi * x)) * (fabs(x) >= R(HW) ? R(0) : R(0.5) * (R(1) + c_w));
+        if (LANCZOS) w = fabs(x) >= R(HW) ? R(0) : sg * s_w * rx * rx;
+        else w = fabs(x) >= R(HW) ? R(0) : sg * (R(1) + c_w) * rx;
         acc += sample_at<AMP, R>(row, i) * w;
         norm += w;
     };
     if (!LANCZOS) {   // one chain, k = -HW+1 .. HW, window angle dropping by pi / HW per tap
         R s_w, c_w;
-        sincospi_r((frac + (R)(HW - 1)) / (R)HW, &s_w, &c_w);
-        R s_k = ((HW - 1) & 1) ? -s_f : s_f;
+        sincospi_r((frac + (R)(HW - 1)) * (R(1) / (R)HW), &s_w, &c_w);
+        R sg = ((HW - 1) & 1) ? R(-1) : R(1);
 #pragma unroll
         for (int k = -HW + 1; k <= HW; ++k) {
-            tap(k, s_k, s_w, c_w);
+            tap(k, sg, s_w, c_w);
             const R c_n = c_w * cos_d + s_w * sin_d;
             s_w = s_w * cos_d - c_w * sin_d;
             c_w = c_n;
-            s_k = -s_k;
+            sg = -sg;
         }
     } else {          // k = 0, -1, .., -HW+1 (angle growing), then k = 1, .., HW (angle dropping)
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
             const R sin_a = side ? -sin_d : sin_d;
             R s_w, c_w;
-            sincospi_r((frac - (R)side) / (R)HW, &s_w, &c_w);
-            R s_k = side ? -s_f : s_f;
+            sincospi_r((frac - (R)side) * (R(1) / (R)HW), &s_w, &c_w);
+            R sg = side ? R(-1) : R(1);
 #pragma unroll
             for (int n = 0; n < HW; ++n) {
-                tap(side ? 1 + n : -n, s_k, s_w, c_w);
+                tap(side ? 1 + n : -n, sg, s_w, c_w);
                 const R c_n = c_w * cos_d - s_w * sin_a;
                 s_w = s_w * cos_d + c_w * sin_a;
                 c_w = c_n;
-                s_k = -s_k;
+                sg = -sg;
             }
         }
     }
-    return norm > R(1e-10) ? acc / norm : R(0);
+    return norm != R(0) ? acc * rcp_r(norm) : R(0);
 }
 
 template <int TT>
@@ -187,6 +199,8 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
     const double gmax = P.aa_gmax, fdom = P.aa_fdom;
     const double inv_vw = 1.0 / vw;
     const double taper_start = ap * (1.0 - P.taper);
+    const double inv_taper_w = ap > taper_start ? 1.0 / (ap - taper_start) : 0.0;
+    const double iv2 = 1.0 / (v * v), t0h2 = (t0 * 0.5) * (t0 * 0.5), inv_dt = 1.0 / P.dt_s;
     R sin_d = R(0), cos_d = R(1);
     if (HW > 0) sincospi_r(R(1) / (R)HW, &sin_d, &cos_d);
 
@@ -235,9 +249,11 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             case TT_CURVED: T = tt_of<TT_CURVED>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
             case TT_VTI: T = tt_of<TT_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
             case TT_CURVED_VTI: T = tt_of<TT_CURVED_VTI>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
-            default: T = tt_of<TT_STRAIGHT>(t0, ds2, dr2, v, eta, P.cr_v0, P.cr_k); break;
+            default:   // the straight legs with this thread's 1/v^2 and the Newton-refined sqrt
+                T = sqrt_newton(fma(ds2, iv2, t0h2)) + sqrt_newton(fma(dr2, iv2, t0h2));
+                break;
             }
-            const double s = (T - P.tstart_s) / P.dt_s;
+            const double s = (T - P.tstart_s) * inv_dt;
             if (!(s >= 0.0 && s < (double)(P.ns - 1))) continue;
             const unsigned char *row =
                 reinterpret_cast<const unsigned char *>(P.amps) + ((int64_t)S.tr[j] * P.amp_stride) * (int64_t)P.elem;
@@ -246,7 +262,7 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             else amp = interpolate_narrow<AMP, R>(row, P.ns, s, method);
             R w = (R)S.w[j];
             if (dj > taper_start) {
-                const R x = (R)((dj - taper_start) / (ap - taper_start));
+                const R x = (R)((dj - taper_start) * inv_taper_w);
                 R cw;
                 if constexpr (sizeof(R) == 8) cw = cospi(x);
                 else cw = cospif(x);
@@ -256,7 +272,7 @@ __global__ void __launch_bounds__(kInterpThreads, PSTM_INTERP_MIN_CTAS) migrate_
             // spreading and obliquity terms: sin = m / (v T), f_max = min(v /
             // (4 gmax sin), 500 Hz) so f_dom / f_max = f_dom max(4 gmax sin / v,
             // 1 / 500), spreading 1 / (v T), obliquity t0 / T.
-            const R Tr = (R)T, inv_T = R(1) / Tr, ivw = (R)inv_vw;
+            const R Tr = (R)T, inv_T = rcp_r(Tr), ivw = (R)inv_vw;
             if (P.aa && T >= 0.001) {
                 const R st = fmin((R)S.m[j] * inv_T * ivw, R(1));
                 if (st >= R(0.01))
