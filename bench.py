@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--dtype", choices=["f32", "bf16", "f16"], default="f32")
-    ap.add_argument("--precision", choices=["exact", "fast"], default="exact")
+    ap.add_argument("--precision", choices=["exact", "fast", "fp32"], default="exact")
     ap.add_argument("--traces", type=int, default=1 << 20)
     ap.add_argument("--tile", type=int, default=64)
     ap.add_argument("--e2e-steps", type=int, default=0,
@@ -417,9 +417,12 @@ def accuracy_vs_fp64(kernel_factory, sv, cfg, n_tr, amps_host, pillars=2):
 
 def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, world, dist, sv, cfg):
     """Plain form (exact sample index, FP32 traces) and the precision form (FP16
-    traces with a power-of-two scale per trace carried by the trace weight;
-    BF16 beside it): pairs/s on the timed tiles of the full case-2 panel and
-    rel-L2 vs the FP64 oracle on the FP32 traces."""
+    traces with a power-of-two scale per trace carried by the trace weight,
+    FP32 traveltime, sample index and trace-end tests, compensated FP32
+    accumulation; the FP32-arithmetic kernel on FP32 traces, FP16 with the
+    FP64 sample index or with FP64 trace-end re-decisions, and BF16 beside
+    it): pairs/s on the timed tiles of the full case-2 panel and rel-L2 vs
+    the FP64 oracle on the FP32 traces."""
     import dataclasses
     import torch
     from oracle import oracle
@@ -429,7 +432,8 @@ def measure_forms(args, k_plain, tb, amps, tile_args, my_tiles, pairs_per_step, 
     n_acc = 1 << 17
     amps_host = amps[:n_acc].float().cpu().numpy()
     res = {}
-    specs = [("plain_exact_f32", "f32", "exact"), ("precision_f16_exact", "f16", "exact"),
+    specs = [("plain_exact_f32", "f32", "exact"), ("precision_f16_fp32", "f16", "fp32"),
+             ("fp32_arithmetic_f32", "f32", "fp32"), ("precision_f16_exact", "f16", "exact"),
              ("precision_f16_fast", "f16", "fast"), ("precision_bf16_fast", "bf16", "fast")]
     f32_tb = tb if amps.dtype == torch.float32 else dataclasses.replace(tb, amplitudes=amps.float())
     f16_tb = None

@@ -43,11 +43,15 @@ typedef enum {
 
 typedef enum { PSTM_AMP_F32 = 0, PSTM_AMP_BF16 = 1, PSTM_AMP_F16 = 2 } pstm_amp_dtype;
 
-/* Traveltime arithmetic of the straight-ray kernel.  EXACT forms the
- * fractional sample index in FP64 (the reference Numba path's precision for
- * the interpolation position and the trace-end test); FAST uses FP32
- * traveltime (the precision form).  Weights and accumulation are FP32 in both. */
-typedef enum { PSTM_PREC_EXACT = 0, PSTM_PREC_FAST = 1 } pstm_precision;
+/* Traveltime arithmetic of the gather kernels (every traveltime kind).  EXACT
+ * forms the fractional sample index in FP64 (the reference Numba path's
+ * precision for the interpolation position and the trace-end test).  FAST
+ * uses FP32 traveltime and re-takes in FP64 the trace-end tests that fall
+ * within 0.01 samples of a trace end.  FP32 is FP32 throughout: traveltime,
+ * sample index and trace-end tests, with FP64 only in the coordinate
+ * differences of the (pillar, trace) records and the fold test (the
+ * precision form's arithmetic).  Weights and accumulation are FP32 in all. */
+typedef enum { PSTM_PREC_EXACT = 0, PSTM_PREC_FAST = 1, PSTM_PREC_FP32 = 2 } pstm_precision;
 typedef enum { PSTM_IMAGE_F64 = 0, PSTM_IMAGE_F32 = 1 } pstm_image_dtype;
 
 /* Trace interpolators of pstm/kernels/interpolation.py:26-301 (linear is 0
@@ -121,7 +125,7 @@ typedef struct {
     int32_t eta_is_3d;
     int32_t compensated;          /* 1: compensated (TwoSum) FP32 accumulation */
     double eta_constant;
-    int32_t precision;            /* pstm_precision; straight rays only, others are FP32 */
+    int32_t precision;            /* pstm_precision */
     int32_t interpolation;        /* pstm_interp; KernelConfig.interpolation_method, base.py:213 */
 } pstm_params;
 

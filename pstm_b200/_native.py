@@ -26,7 +26,7 @@ STATUS_NAMES = {
 AMP_F32, AMP_BF16, AMP_F16 = 0, 1, 2
 IMAGE_F64, IMAGE_F32 = 0, 1
 TT_STRAIGHT, TT_CURVED, TT_VTI, TT_CURVED_VTI = 0, 1, 2, 3
-PREC_EXACT, PREC_FAST = 0, 1
+PREC_EXACT, PREC_FAST, PREC_FP32 = 0, 1, 2
 # pstm_interp, named as KernelConfig.interpolation_method (aliases of interpolation.py:42-51)
 INTERP_BY_NAME = {"linear": 0, "nearest": 1, "cubic": 2, "sinc4": 3, "sinc8": 4, "sinc16": 5,
                   "lanczos3": 6, "lanczos5": 7}

@@ -35,6 +35,7 @@ struct BatchPlan {
     Launch L;
     int tt = 0, amp = 0;
     bool per_pillar = false, exact = false;
+    int prec = PSTM_PREC_EXACT;   // pstm_precision
     int64_t n_p = 0;
     std::vector<BinWork> work;   // non-empty bins, most traces first
 };
@@ -130,6 +131,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     bp.amp = tr->amp_dtype;
     bp.per_pillar = vel->is_3d || (prm->eta && prm->eta_is_3d);
     bp.exact = prm->precision == PSTM_PREC_EXACT;
+    bp.prec = prm->precision;
     P.exact_units = bp.exact ? 1 : 0;
     P.curved_kind = (prm->traveltime == PSTM_TT_CURVED || prm->traveltime == PSTM_TT_CURVED_VTI) ? 1 : 0;
     bp.n_p = bp.per_pillar ? (int64_t)out->nx * out->ny : 1;
@@ -191,7 +193,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
     unsigned ctas = 0;
     bp.L.configure_only = true;
     bp.L.ctas_out = &ctas;
-    e = launch_kind(bp.tt, P, reinterpret_cast<const KParams *>(c->kparams.ptr), bp.amp, bp.per_pillar, bp.exact,
+    e = launch_kind(bp.tt, P, reinterpret_cast<const KParams *>(c->kparams.ptr), bp.amp, bp.per_pillar, bp.prec,
                     bp.L);
     if (e != cudaSuccess) return cuda_fail(c, e, "configuring the persistent kernel");
     bp.L.configure_only = false;
@@ -234,7 +236,7 @@ int32_t enqueue_batch(Ctx *c, BatchPlan &bp, cudaStream_t st) {
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(c, e, "store_bins launch");
     }
     bp.L.stream = st;
-    e = launch_kind(bp.tt, P, reinterpret_cast<const KParams *>(c->kparams.ptr), bp.amp, bp.per_pillar, bp.exact,
+    e = launch_kind(bp.tt, P, reinterpret_cast<const KParams *>(c->kparams.ptr), bp.amp, bp.per_pillar, bp.prec,
                     bp.L);
     if (e != cudaSuccess) return cuda_fail(c, e, "persistent migrate kernel launch");
     return PSTM_OK;
@@ -250,7 +252,7 @@ std::vector<unsigned char> graph_key(const BatchPlan &bp) {
     };
     put(&bp.P, sizeof(KParams));
     if (!bp.work.empty()) put(bp.work.data(), bp.work.size() * sizeof(BinWork));
-    const int64_t extra[8] = {bp.tt, bp.amp, bp.per_pillar, bp.exact, (int64_t)bp.L.grid.x, (int64_t)bp.L.smem,
+    const int64_t extra[8] = {bp.tt, bp.amp, bp.per_pillar, bp.prec, (int64_t)bp.L.grid.x, (int64_t)bp.L.smem,
                               (int64_t)(uintptr_t)bp.L.bins, (int64_t)(uintptr_t)bp.L.counter};
     put(extra, sizeof(extra));
     return k;

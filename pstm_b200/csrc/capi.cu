@@ -171,6 +171,7 @@ int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc 
     tp.amp = tr->amp_dtype;
     tp.per_pillar = per_pillar;
     tp.exact = exact;
+    tp.prec = prm->precision;
     tp.n_p = n_p;
     tp.empty = false;
     return PSTM_OK;
@@ -212,7 +213,7 @@ int32_t launch_items(Ctx *c, const TilePlan &tp, const std::vector<BinWork> &w) 
     L.bins = reinterpret_cast<const BinWork *>(c->seg_bins.ptr);
     L.n_bins = (int)w.size();
     L.counter = reinterpret_cast<unsigned long long *>(c->seg_counter.ptr);
-    e = launch_kind(tp.tt, P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, L);
+    e = launch_kind(tp.tt, P, tp.Pg, tp.amp, tp.per_pillar, tp.prec, L);
     return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "segmented migrate kernel launch");
 }
 
@@ -230,7 +231,7 @@ int32_t launch_tile(Ctx *c, const TilePlan &tp) {
         append_segments(w, 0, P0.n_traces, segment_traces(c, P0), P0.image, P0.fold);
         return launch_items(c, tp, w);
     }
-    const cudaError_t e = launch_kind(tp.tt, tp.P, tp.Pg, tp.amp, tp.per_pillar, tp.exact, tp.L);
+    const cudaError_t e = launch_kind(tp.tt, tp.P, tp.Pg, tp.amp, tp.per_pillar, tp.prec, tp.L);
     return e == cudaSuccess ? PSTM_OK : cuda_fail(c, e, "migrate kernel launch");
 }
 

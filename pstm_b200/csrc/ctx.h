@@ -54,6 +54,7 @@ struct TilePlan {
     Launch L;
     int tt = 0, amp = 0;
     bool per_pillar = false, exact = false;
+    int prec = PSTM_PREC_EXACT;   // pstm_precision of the launch
     int64_t n_p = 0;
     bool empty = true;   // no traces: nothing to launch
 };

@@ -27,24 +27,25 @@ struct Launch {
 };
 
 template <int TT>
-cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact, const Launch &L);
+cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, int prec, const Launch &L);
 // each kind is instantiated in its own migrate_k<kind>.cu, nowhere else
-extern template cudaError_t launch_migrate<TT_STRAIGHT>(const KParams &, const KParams *, int, bool, bool,
+extern template cudaError_t launch_migrate<TT_STRAIGHT>(const KParams &, const KParams *, int, bool, int,
                                                         const Launch &);
-extern template cudaError_t launch_migrate<TT_CURVED>(const KParams &, const KParams *, int, bool, bool,
+extern template cudaError_t launch_migrate<TT_CURVED>(const KParams &, const KParams *, int, bool, int,
                                                       const Launch &);
-extern template cudaError_t launch_migrate<TT_VTI>(const KParams &, const KParams *, int, bool, bool, const Launch &);
-extern template cudaError_t launch_migrate<TT_CURVED_VTI>(const KParams &, const KParams *, int, bool, bool,
+extern template cudaError_t launch_migrate<TT_VTI>(const KParams &, const KParams *, int, bool, int, const Launch &);
+extern template cudaError_t launch_migrate<TT_CURVED_VTI>(const KParams &, const KParams *, int, bool, int,
                                                           const Launch &);
 
-// exact selects the FP64 sample-index path.
-inline cudaError_t launch_kind(int traveltime, const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact,
+// prec (pstm_precision) selects the FP64 sample-index path, FP32 traveltime
+// with FP64 trace-end re-decisions, or FP32 throughout.
+inline cudaError_t launch_kind(int traveltime, const KParams &P, const KParams *Pg, int amp, bool vel3d, int prec,
                                const Launch &L) {
     switch (traveltime) {
-    case PSTM_TT_STRAIGHT: return launch_migrate<TT_STRAIGHT>(P, Pg, amp, vel3d, exact, L);
-    case PSTM_TT_CURVED: return launch_migrate<TT_CURVED>(P, Pg, amp, vel3d, exact, L);
-    case PSTM_TT_VTI: return launch_migrate<TT_VTI>(P, Pg, amp, vel3d, exact, L);
-    default: return launch_migrate<TT_CURVED_VTI>(P, Pg, amp, vel3d, exact, L);
+    case PSTM_TT_STRAIGHT: return launch_migrate<TT_STRAIGHT>(P, Pg, amp, vel3d, prec, L);
+    case PSTM_TT_CURVED: return launch_migrate<TT_CURVED>(P, Pg, amp, vel3d, prec, L);
+    case PSTM_TT_VTI: return launch_migrate<TT_VTI>(P, Pg, amp, vel3d, prec, L);
+    default: return launch_migrate<TT_CURVED_VTI>(P, Pg, amp, vel3d, prec, L);
     }
 }
 

@@ -470,8 +470,10 @@ struct CtaShared {
 // (it selects the buffer and the mbarrier phase of every chunk).  Returns
 // false when a bounded wait gave up.
 // W2: spreading and obliquity both on (the common case), else the weight
-// exponent is chosen at run time.
-template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+// exponent is chosen at run time.  GUARD (FP32-traveltime path only): trace-end
+// tests within 0.01 samples of a trace end are re-taken in FP64; without it
+// (PSTM_PREC_FP32) they are FP32 like the rest of the sample index.
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2, bool GUARD>
 __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__restrict__ Pg, const Item &it,
                                              unsigned char *smem, CtaShared &sh, int64_t &chunk_base) {
     constexpr bool HAS_C = RecLayout<TT>::kHasC;
@@ -750,7 +752,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     const float4 A = recA[ri];
                     bool act = ALLIN ? true : (A.x <= s.ap);
                     const int roff = __float_as_int(A.w);   // row offset; the trace is roff / row_bytes
-                    if (HARD && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
+                    if (HARD && (EXACT || GUARD) && A.x == s.ap)   // FP32 tie of distance and aperture: decide in FP64
                         act = !exact_outside_aperture(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q], s_oy[q]);
                     float T, f;
                     int i0;
@@ -781,20 +783,28 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         T = traveltime<TT>(P, ts, s, B, Cc);
                         if constexpr (TT != TT_STRAIGHT) T = ts.tz ? 0.f : T;
                         float sidx = fmaf(T, s_scale, s_offset);
-                        // T = 0 exactly: the FP64 decision is known per time, no guard band
-                        const float x = fabsf(sidx - g_mid);
-                        const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
-                        const bool band = act && !fast_ok && !ts.tz && x <= g_out;
-                        if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
-                        if constexpr (SLOW) {   // re-decide the guard band in FP64
-                            ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q],
-                                                             s_oy[q]);
-                            sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
-                        } else {
-                            ok = act && fast_ok;
-                            pmask |= band ? (1u << c) : 0u;
+                        if constexpr (GUARD) {
+                            // T = 0 exactly: the FP64 decision is known per time, no guard band
+                            const float x = fabsf(sidx - g_mid);
+                            const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
+                            const bool band = act && !fast_ok && !ts.tz && x <= g_out;
+                            if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
+                            if constexpr (SLOW) {   // re-decide the guard band in FP64
+                                ok = band && exact_sample_ok<TT>(Pg, it.trace0 + c0 + roff / row_bytes, p, t, s_ox[q],
+                                                                 s_oy[q]);
+                                sidx = fminf(fmaxf(sidx, 0.f), s_clamp);
+                            } else {
+                                ok = act && fast_ok;
+                                pmask |= band ? (1u << c) : 0u;
+                            }
+                            sidx = ok ? sidx : 0.f;
+                        } else {   // FP32 trace-end test: the index is inside iff clamping leaves it unchanged
+                            const float sc = fminf(fmaxf(sidx, 0.f), s_clamp);   // (NaN -> 0, outside)
+                            bool in = sc == sidx;
+                            if constexpr (TT != TT_STRAIGHT) in = ts.tz ? ts.tz_in : in;
+                            ok = act && in;
+                            sidx = sc;
                         }
-                        sidx = ok ? sidx : 0.f;
                         const float fl = __fadd_rd(sidx, 8388608.f);
                         i0 = __float_as_int(fl) - 0x4B000000;
                         f = sidx - (fl - 8388608.f);
@@ -859,13 +869,21 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                         T = traveltime<TT>(P, ts, s, B, Cc);
                         if constexpr (TT != TT_STRAIGHT) T = ts.tz ? 0.f : T;
                         float sidx = fmaf(T, s_scale, s_offset);
-                        const float x = fabsf(sidx - g_mid);
-                        const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
-                        const bool band = !fast_ok && !ts.tz && x <= g_out;
-                        if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
-                        ok = fast_ok;
-                        pmask |= band ? (1u << c) : 0u;
-                        sidx = ok ? sidx : 0.f;
+                        if constexpr (GUARD) {
+                            const float x = fabsf(sidx - g_mid);
+                            const bool fast_ok = ts.tz ? ts.tz_in : (x <= g_in);
+                            const bool band = !fast_ok && !ts.tz && x <= g_out;
+                            if constexpr (TT != TT_STRAIGHT) sidx = ts.tz ? fminf(fmaxf(sidx, 0.f), s_clamp) : sidx;
+                            ok = fast_ok;
+                            pmask |= band ? (1u << c) : 0u;
+                            sidx = ok ? sidx : 0.f;
+                        } else {   // FP32 trace-end test, as in `pair`
+                            const float sc = fminf(fmaxf(sidx, 0.f), s_clamp);
+                            bool in = sc == sidx;
+                            if constexpr (TT != TT_STRAIGHT) in = ts.tz ? ts.tz_in : in;
+                            ok = in;
+                            sidx = sc;
+                        }
                         const float fl = __fadd_rd(sidx, 8388608.f);
                         i0 = __float_as_int(fl) - 0x4B000000;
                         f = sidx - (fl - 8388608.f);
@@ -928,7 +946,7 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                     PSTM_UNROLL(PSTM_UNROLL_TAPER)
                     for (int c = 0; c < n; ++c) a += pair(c, F{}, F{}, Tr{}, Tr{}, F{});
                 }
-                if constexpr (!EXACT) {   // second pass over the flagged records only
+                if constexpr (!EXACT && GUARD) {   // second pass over the flagged records only
                     unsigned m = __reduce_or_sync(0xffffffffu, pmask);
                     while (m) {
                         const int c = __ffs(m) - 1;
@@ -1018,7 +1036,7 @@ __device__ __forceinline__ void init_barriers(CtaShared &sh) {
 }
 
 // One CTA per (pillar block, time block) of one tile.
-template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2, bool GUARD>
 __global__ void __launch_bounds__(kThreads, 1)
 migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     static_assert(kMaxPB <= kThreads / 32, "one warp per pillar builds the records");
@@ -1036,7 +1054,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
     it.pby = blockIdx.x - it.pbx * P.n_pblk_y;
     it.tblock = blockIdx.y;
     int64_t chunk_base = 0;
-    migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base);
+    migrate_item<TT, AMP, VEL3D, EXACT, W2, GUARD>(P, Pg, it, smem, sh, chunk_base);
 }
 
 // Persistent form for many outputs (offset bins): one CTA per SM fetches
@@ -1045,7 +1063,7 @@ migrate_kernel(const KParams P, const KParams *__restrict__ Pg) {
 // schedule (sw.boxes non-null) the items are (segment, pillar block, time
 // block) of P.image / P.fold, numbered segment by segment; an item finds its
 // segment by binary search in the segments' inclusive prefix counts.
-template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2, bool GUARD>
 __global__ void __launch_bounds__(kThreads, 1)
 migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const BinWork *__restrict__ bins,
                           int n_bins, unsigned long long *work_counter, const ScatterWork sw) {
@@ -1089,7 +1107,7 @@ migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const
             it.geo = P.geo + it.trace0 * kGeoDoubles;
             it.image = P.image;
             it.fold = P.fold;
-            if (!migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base)) break;
+            if (!migrate_item<TT, AMP, VEL3D, EXACT, W2, GUARD>(P, Pg, it, smem, sh, chunk_base)) break;
             continue;
         }
         const BinWork &bw = bins[item / per_bin];
@@ -1105,7 +1123,7 @@ migrate_persistent_kernel(const KParams P, const KParams *__restrict__ Pg, const
         it.geo = P.geo + bw.trace0 * kGeoDoubles;
         it.image = bw.image;
         it.fold = bw.fold;
-        if (!migrate_item<TT, AMP, VEL3D, EXACT, W2>(P, Pg, it, smem, sh, chunk_base)) break;
+        if (!migrate_item<TT, AMP, VEL3D, EXACT, W2, GUARD>(P, Pg, it, smem, sh, chunk_base)) break;
     }
 }
 

@@ -33,17 +33,17 @@ static cudaError_t opt_in_smem(SmemOptIn &state, Kernel kern, size_t smem) {
     return e;
 }
 
-template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2>
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool W2, bool GUARD>
 static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L) {
     if (!L.bins && !L.scatter.boxes) {
-        auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2>;
+        auto kern = migrate_kernel<TT, AMP, VEL3D, EXACT, W2, GUARD>;
         static SmemOptIn opt_in;   // per instantiation
         cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
         if (e != cudaSuccess) return e;
         kern<<<L.grid, kThreads, L.smem, L.stream>>>(P, Pg);
         return cudaGetLastError();
     }
-    auto kern = migrate_persistent_kernel<TT, AMP, VEL3D, EXACT, W2>;
+    auto kern = migrate_persistent_kernel<TT, AMP, VEL3D, EXACT, W2, GUARD>;
     static SmemOptIn opt_in;
     {
         cudaError_t e = opt_in_smem(opt_in, kern, L.smem);
@@ -66,16 +66,16 @@ static cudaError_t launch_w(const KParams &P, const KParams *Pg, const Launch &L
     return cudaGetLastError();
 }
 
-template <int TT, int AMP, bool VEL3D, bool EXACT>
+template <int TT, int AMP, bool VEL3D, bool EXACT, bool GUARD>
 static cudaError_t launch_one(const KParams &P, const KParams *Pg, const Launch &L) {
-    if (P.spreading && P.obliquity) return launch_w<TT, AMP, VEL3D, EXACT, true>(P, Pg, L);
-    return launch_w<TT, AMP, VEL3D, EXACT, false>(P, Pg, L);
+    if (P.spreading && P.obliquity) return launch_w<TT, AMP, VEL3D, EXACT, true, GUARD>(P, Pg, L);
+    return launch_w<TT, AMP, VEL3D, EXACT, false, GUARD>(P, Pg, L);
 }
 
-template <int TT, bool EXACT>
+template <int TT, bool EXACT, bool GUARD>
 static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, bool vel3d, const Launch &L) {
 #define PSTM_CASE(A_, V_) \
-    if (amp == A_ && vel3d == V_) return launch_one<TT, A_, V_, EXACT>(P, Pg, L);
+    if (amp == A_ && vel3d == V_) return launch_one<TT, A_, V_, EXACT, GUARD>(P, Pg, L);
     PSTM_CASE(AMP_F32, false) PSTM_CASE(AMP_F32, true)
     PSTM_CASE(AMP_BF16, false) PSTM_CASE(AMP_BF16, true)
     PSTM_CASE(AMP_F16, false) PSTM_CASE(AMP_F16, true)
@@ -83,11 +83,14 @@ static cudaError_t launch_prec(const KParams &P, const KParams *Pg, int amp, boo
     return cudaErrorInvalidValue;
 }
 
-// exact: FP64 sample index; otherwise FP32 traveltime.
+// prec: PSTM_PREC_EXACT the FP64 sample index; PSTM_PREC_FAST FP32 traveltime with
+// FP64 re-decisions of the trace-end tests in a guard band; PSTM_PREC_FP32 FP32
+// traveltime, sample index and trace-end tests (no guard band).
 template <int TT>
-cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, bool exact, const Launch &L) {
-    if (exact) return launch_prec<TT, true>(P, Pg, amp, vel3d, L);
-    return launch_prec<TT, false>(P, Pg, amp, vel3d, L);
+cudaError_t launch_migrate(const KParams &P, const KParams *Pg, int amp, bool vel3d, int prec, const Launch &L) {
+    if (prec == PSTM_PREC_EXACT) return launch_prec<TT, true, true>(P, Pg, amp, vel3d, L);
+    if (prec == PSTM_PREC_FAST) return launch_prec<TT, false, true>(P, Pg, amp, vel3d, L);
+    return launch_prec<TT, false, false>(P, Pg, amp, vel3d, L);
 }
 
 }  // namespace pstm

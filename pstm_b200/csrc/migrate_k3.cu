@@ -1,5 +1,5 @@
 // Instantiations of the gather kernel for traveltime kind 3.
 #include "migrate_dispatch.cuh"
 namespace pstm {
-template cudaError_t launch_migrate<3>(const KParams &, const KParams *, int, bool, bool, const Launch &);
+template cudaError_t launch_migrate<3>(const KParams &, const KParams *, int, bool, int, const Launch &);
 }

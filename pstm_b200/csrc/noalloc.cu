@@ -184,7 +184,7 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     L.grid = dim3((unsigned)nblk_p, (unsigned)nblk_t);
     L.smem = smem;
     L.stream = st;
-    e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, exact, L);
+    e = launch_kind(prm->traveltime, P, Pg, tr->amp_dtype, per_pillar, prm->precision, L);
     if (e != cudaSuccess) return cuda_fail(e, "migrate kernel launch");
     return PSTM_OK;
 }

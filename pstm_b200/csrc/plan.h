@@ -53,7 +53,7 @@ inline int32_t check_args(const pstm_traces_desc *tr, const pstm_output_desc *ou
     if (!vel->vrms) return fail(PSTM_ERR_INVALID_ARGUMENT, "null velocity");
     if (prm->traveltime < PSTM_TT_STRAIGHT || prm->traveltime > PSTM_TT_CURVED_VTI)
         return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown traveltime kind");
-    if (prm->precision != PSTM_PREC_EXACT && prm->precision != PSTM_PREC_FAST)
+    if (prm->precision != PSTM_PREC_EXACT && prm->precision != PSTM_PREC_FAST && prm->precision != PSTM_PREC_FP32)
         return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown precision");
     if (prm->interpolation < PSTM_INTERP_LINEAR || prm->interpolation > PSTM_INTERP_LANCZOS5)
         return fail(PSTM_ERR_INVALID_ARGUMENT, "unknown interpolation method");

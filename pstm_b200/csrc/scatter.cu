@@ -186,7 +186,7 @@ extern "C" int32_t pstm_cuda_migrate_scatter_dev(void *ctx, const pstm_traces_de
     L.stream = st;
     L.counter = reinterpret_cast<unsigned long long *>(c->seg_counter.ptr);
     L.scatter = ScatterWork{boxes, ends, n_seg, S};
-    e = launch_kind(tp.tt, Pa, tp.Pg, tp.amp, tp.per_pillar, tp.exact, L);
+    e = launch_kind(tp.tt, Pa, tp.Pg, tp.amp, tp.per_pillar, tp.prec, L);
     if (e != cudaSuccess) return cuda_fail(c, e, "scatter migrate launch");
     if (n_items_out) {   // diagnostics: the schedule's item count (synchronises the stream)
         long long total = 0;

@@ -104,9 +104,12 @@ class CudaKernel:
         Metal host rule (``metal_compiled.py:631-664``): the centre pillar is
         used for every pillar unless the lateral variation exceeds 5 %.
     precision:
-        ``"exact"`` forms the straight-ray sample index in FP64 (the reference
-        Numba path's interpolation position); ``"fast"`` uses FP32 traveltime
-        (the precision form).  Curved-ray and VTI kernels are FP32 either way.
+        ``"exact"`` forms the sample index in FP64 (the reference Numba path's
+        interpolation position and trace-end test); ``"fast"`` uses FP32
+        traveltime and re-takes in FP64 the trace-end tests within 0.01
+        samples of a trace end; ``"fp32"`` is FP32 throughout (traveltime,
+        sample index, trace-end tests), FP64 staying in the coordinate
+        differences and the fold test: the precision form's arithmetic.
     """
 
     def __init__(self, device: int | None = None, trace_dtype: str = "auto",
@@ -117,9 +120,10 @@ class CudaKernel:
             raise ValueError("compensated must be 'auto', True or False")
         self._compensated = compensated
         self._velocity_mode = velocity_mode
-        if precision not in ("exact", "fast"):
-            raise ValueError("precision must be 'exact' or 'fast'")
-        self._precision = nat.PREC_EXACT if precision == "exact" else nat.PREC_FAST
+        modes = {"exact": nat.PREC_EXACT, "fast": nat.PREC_FAST, "fp32": nat.PREC_FP32}
+        if precision not in modes:
+            raise ValueError("precision must be 'exact', 'fast' or 'fp32'")
+        self._precision = modes[precision]
         self._config = None
         self._ctx = None
         self._lib = None

@@ -3,7 +3,8 @@
 Tolerances (written here, checked below):
 * plain straight-ray, FP32 traces (FP64 sample index, the default), vs the
   reference Numba path: fold bit-exact, image relative L2 <= 1e-5;
-* the precision form (FP32 traveltime, "fast"): <= 1e-3 against the FP64 oracle;
+* the precision form (FP32 traveltime, "fast" with FP64 trace-end re-decisions, "fp32"
+  without): <= 1e-3 against the FP64 oracle;
 * curved / VTI / curved+VTI / AA / 3-D velocity, FP32 traces, vs the FP64
   oracle: fold bit-exact, image relative L2 <= 1e-5 on the FP64 sample-index
   path ("exact", the default) and <= 1e-4 with FP32 traveltime ("fast");
@@ -102,7 +103,7 @@ def test_device_tensors_match_host_arrays(cuda_kernel_factory):
     np.testing.assert_array_equal(dout.image.cpu().numpy(), o.image)
 
 
-@pytest.mark.parametrize("precision", ["exact", "fast"])
+@pytest.mark.parametrize("precision", ["exact", "fast", "fp32"])
 @pytest.mark.parametrize("kind", ["straight_ray", "curved_ray", "anisotropic_vti", "curved_vti"])
 @pytest.mark.parametrize("aa", [False, True])
 def test_traveltime_kinds_vs_oracle(kind, aa, precision, cuda_kernel_factory):
@@ -121,7 +122,7 @@ def test_traveltime_kinds_vs_oracle(kind, aa, precision, cuda_kernel_factory):
     assert err <= tol, err
 
 
-@pytest.mark.parametrize("precision", ["exact", "fast"])
+@pytest.mark.parametrize("precision", ["exact", "fast", "fp32"])
 def test_curved_zero_gradient_and_constant_eta(precision, cuda_kernel_factory):
     from pstm_b200 import workloads
     case = workloads.config2_small(n_traces=1024, nx=8, ny=8)
@@ -147,7 +148,7 @@ def test_curved_zero_gradient_and_constant_eta(precision, cuda_kernel_factory):
     assert rel_l2(out3.image, ref3.image) <= tol
 
 
-@pytest.mark.parametrize("precision", ["exact", "fast"])
+@pytest.mark.parametrize("precision", ["exact", "fast", "fp32"])
 @pytest.mark.parametrize("dtype", ["bf16", "f16"])
 def test_16bit_traces(dtype, precision, cuda_kernel_factory):
     from pstm_b200 import workloads
@@ -187,7 +188,7 @@ def _noise_tile(n_traces=16384, pillars=8, seed=3):
     return sv.trace_block(), out, vel, workloads.survey_config(aa=True)
 
 
-@pytest.mark.parametrize("precision", ["exact", "fast"])
+@pytest.mark.parametrize("precision", ["exact", "fast", "fp32"])
 def test_precision_form_noise_dominated_config2_tile(precision, cuda_kernel_factory):
     from pstm_b200.cuda_kernel import bf16_bits_to_float32, float32_to_bf16_bits
     tb, out, vel, cfg = _noise_tile()
@@ -230,11 +231,13 @@ def test_f16_panel_device_matches_host_rule(cuda_kernel_factory):
     np.testing.assert_array_equal(d16.weights.cpu().numpy(), w * inv)
 
 
+@pytest.mark.parametrize("precision", ["fast", "fp32"])
 @pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p)[6:-4])
-def test_fast_precision_form_on_golden(path, cuda_kernel_factory):
-    """FP32 traveltime (the precision form) against the reference outputs."""
+def test_fast_precision_form_on_golden(path, precision, cuda_kernel_factory):
+    """FP32 traveltime (with and without the FP64 trace-end re-decisions)
+    against the reference outputs."""
     tb, out, vel, cfg, img_ref, fold_ref = load_golden_case(path)
-    k = cuda_kernel_factory(cfg, precision="fast")
+    k = cuda_kernel_factory(cfg, precision=precision)
     k.migrate_tile(tb, out, vel)
     np.testing.assert_array_equal(out.fold, fold_ref)
     if np.abs(img_ref).max() > 0:

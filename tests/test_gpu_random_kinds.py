@@ -7,8 +7,9 @@ trace weights or none, sample rate and start time, 1-D or 3-D velocity, eta
 as a constant or a function of t0, the curved-ray gradient (0 included) and a
 2-D or 3-D fold; traces are band-limited noise.  On the FP64 sample-index path
 ("exact") the image must be within 1e-5 relative L2 of the oracle and the fold
-identical; with FP32 traveltime ("fast") within 1e-4 (on noise-like traces FP32
-traveltime alone leaves ~1.1e-5, even for straight rays)."""
+identical; with FP32 traveltime ("fast", and "fp32" whose trace-end tests are
+FP32 too) within 1e-4 (on noise-like traces FP32 traveltime alone leaves
+~1.1e-5, even for straight rays)."""
 from __future__ import annotations
 
 import numpy as np
@@ -65,7 +66,7 @@ def _draw(seed):
     return kind, tb, out, vel, cfg
 
 
-@pytest.mark.parametrize("precision", ["exact", "fast"])
+@pytest.mark.parametrize("precision", ["exact", "fast", "fp32"])
 @pytest.mark.parametrize("seed", range(12))
 def test_random_configuration_vs_oracle(seed, precision, cuda_kernel_factory):
     from pstm_b200.base import OutputTile
