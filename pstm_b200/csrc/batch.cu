@@ -115,7 +115,7 @@ int32_t plan_batch(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc *o
         PB = force->pb;
         chunk = force->chunk;
     } else {
-        plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB);
+        plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB, tr->amp_dtype);
         auto it = c->tuned.find(class_key(tr, out, vel, prm));
         if (it != c->tuned.end() && !c->force_r && !c->force_pb) {
             R = it->second.r;
@@ -381,7 +381,7 @@ int32_t pstm_cuda_autotune_bins(void *ctx, const pstm_traces_desc *traces, const
     // candidates: the default shape first, then pillars per CTA x times per
     // lane x panel depth
     Shape def;
-    plan::choose_shape(o.nt, 0, 0, def.r, def.pb);
+    plan::choose_shape(o.nt, 0, 0, def.r, def.pb, traces->amp_dtype);
     std::vector<Shape> cand{def};
     std::vector<int> rs{def.r};
     if (def.r > 1) rs.push_back((def.r + 1) / 2);

@@ -94,7 +94,7 @@ int32_t prepare_tile(Ctx *c, const pstm_traces_desc *tr, const pstm_output_desc 
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
     int R, PB;
-    plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB);
+    plan::choose_shape(out->nt, c->force_r, c->force_pb, R, PB, tr->amp_dtype);
     KParams &P = tp.P;
     P = make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // nothing to add: image += 0, fold += 0

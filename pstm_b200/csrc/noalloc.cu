@@ -135,7 +135,7 @@ extern "C" int32_t pstm_cuda_migrate_tile_noalloc(const pstm_traces_desc *tr, co
     cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : cudaStreamLegacy;
 
     int R, PB;
-    plan::choose_shape(out->nt, 0, 0, R, PB);
+    plan::choose_shape(out->nt, 0, 0, R, PB, tr->amp_dtype);
     KParams P = plan::make_params(tr, out, vel, prm, PB);
     if (tr->n_traces == 0) return PSTM_OK;   // image += 0, fold += 0
     const bool exact = prm->precision == PSTM_PREC_EXACT;
