@@ -437,10 +437,16 @@ __host__ __device__ constexpr int record_buffer_bytes(int PB, bool has_c) {
     return PB * kMaxChunk * 16 * (has_c ? 3 : 2);
 }
 __host__ __device__ constexpr int geo_buffer_bytes() { return kMaxChunk * kGeoDoubles * 8; }
-// Per-lane FP32 partial sums of one CTA: PB x R x kThreads floats.
-// FP32 partial sums of a CTA, and with compensated accumulation their TwoSum error terms.
+// FP32 partial sums of a CTA (PB x R x kThreads floats), and with compensated
+// accumulation their TwoSum error terms, kept in BF16: an error term needs
+// only a few significant bits (it corrects the partial's last bits), and half
+// the bytes leave more of shared memory to the staged traces.
 __host__ __device__ constexpr int partial_bytes(int PB, int R, bool compensated = false) {
-    return PB * R * kThreads * 4 * (compensated ? 2 : 1);
+    return PB * R * kThreads * (compensated ? 6 : 4);
+}
+__device__ __forceinline__ float bf16_to_f32(unsigned short h) { return __uint_as_float((unsigned)h << 16); }
+__device__ __forceinline__ unsigned short f32_to_bf16(float x) {
+    return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
 
 // ---------------------------------------------------------------- the kernel
@@ -494,7 +500,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     unsigned char *const rec_base = geo_base + 2 * geo_buffer_bytes();
     float *const s_acc = reinterpret_cast<float *>(rec_base + 2 * REC_BYTES);   // [PB][R][kThreads]
     const bool comp = P.compensated != 0;
-    float *const s_err = s_acc + PB * R * kThreads;   // [PB][R][kThreads] when comp
+    unsigned short *const s_err =   // [PB][R][kThreads] BF16 error terms when comp
+        reinterpret_cast<unsigned short *>(s_acc + PB * R * kThreads);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pbx = it.pbx, pby = it.pby;
@@ -528,7 +535,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
     const int64_t n_chunks = (it.n_traces + C - 1) / C;
     const int flush_every = P.flush_every;
 
-    for (int i = tid; i < PB * R * kThreads * (comp ? 2 : 1); i += kThreads) s_acc[i] = 0.f;
+    // partials and (comp) the error terms behind them: PB R kThreads (3/2) floats
+    for (int i = tid; i < PB * R * kThreads * (comp ? 3 : 2) / 2; i += kThreads) s_acc[i] = 0.f;
 
     // one thread: TMA bulk copies of chunk k (packed geometry, and the amplitude
     // rows when they are 16-byte aligned) into buffer b
@@ -665,9 +673,9 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 float &sa = s_acc[(q * R + r) * kThreads + tid];
                 float a = sa;
                 if (comp) {   // the partial and its rounding error, summed in FP32 once more
-                    float &se = s_err[(q * R + r) * kThreads + tid];
-                    a += se;
-                    se = 0.f;
+                    unsigned short &se = s_err[(q * R + r) * kThreads + tid];
+                    a += bf16_to_f32(se);
+                    se = 0;
                 }
                 if (p >= 0 && t < P.nt && a != 0.f) {
                     const int64_t idx = (int64_t)p * P.nt + t;
@@ -957,7 +965,8 @@ __device__ __forceinline__ bool migrate_item(const KParams &P, const KParams *__
                 float &sa = s_acc[(q * R + r) * kThreads + vt];
                 if (comp) {   // TwoSum: sa + a = t + e exactly; the errors are kept apart
                     const float s0 = sa, t = s0 + a, bp = t - s0;
-                    s_err[(q * R + r) * kThreads + vt] += (s0 - (t - bp)) + (a - bp);
+                    unsigned short &se = s_err[(q * R + r) * kThreads + vt];
+                    se = f32_to_bf16(bf16_to_f32(se) + ((s0 - (t - bp)) + (a - bp)));
                     sa = t;
                 } else {
                     sa += a;
